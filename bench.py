@@ -1,0 +1,373 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 engine on the 1M-atom NVE step (one JSON line on rank 0).
+
+Workload: N = 4*64^3 = 1 048 576 atoms, FCC at rho = 0.8442, T = 1.0,
+rc = 2.5, dt = 0.005, seeded Maxwell-Boltzmann velocities (the library's own
+engine::InitialCondition).  A step is one velocity-Verlet step of the whole
+system (kick, drift, wrap, forces, kick) with its ThermodynamicMeasurement.
+
+  value        FP64 drop-in path, atom-steps/s, state resident in HBM, CUDA
+               events on the engine's stream, max over ranks
+  mixed        same for the mixed-precision path (FP32 pair arithmetic)
+  drift        |dE/E| of both paths over --drift-steps steps
+  e2e          FP64 path through the C ABI from pinned host buffers: upload the
+               SystemState, --steps steps with every per-step record read back
+               to the host, download the SystemState
+  roofline     the pair kernel (the dominant one) against the measured FP64 FMA peak
+  cpu_baseline the CPU oracle (the reference's algorithm, its release flags) on
+               the host cores, one 1M-atom system per thread
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import pathlib
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "lennard-jonesium_b200"))
+
+METRIC = "atom-steps/s, 1M-atom LJ: FP32-pair vs FP64 on B200 at equal energy drift"
+UNIT = "atom-steps/s"
+WORK = dict(n_cells=64, T=1.0, rho=0.8442, rc=2.5, dt=0.005, seed=5489)
+N_ATOMS = 4 * WORK["n_cells"] ** 3  # --cells changes it (profiling captures of a smaller case)
+HBM_PEAK = None
+
+
+def workload_config(extra=None):
+    c = {"workload": f"FCC LJ fluid, N={N_ATOMS} (4*{WORK['n_cells']}^3), rho=0.8442, T=1.0, rc=2.5, "
+                     "dt=0.005, seeded MB velocities, spline-truncated LJ, NVE velocity Verlet",
+         "atoms": N_ATOMS, "cutoff": WORK["rc"], "time_delta": WORK["dt"],
+         "l2": "per-step working set (state + neighbour list, > 400 MB) exceeds the 126 MB L2",
+         "parallelism": "replicas only (one independent system per GPU)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {"hbm_gbs": 6650.0, "fallback": True}
+
+
+def alg_flops_per_atom_step(N, L, rc, rho):
+    """Survey-defined algorithmic work of the reference's half-shell algorithm:
+    F = 9 C + 30 P, C = (27 rho a^3 - 1) / 2 candidate tests, P = (2 pi / 3) rho rc^3 pairs."""
+    n_c = math.floor(L / rc)
+    a = L / n_c
+    C = (27 * rho * a ** 3 - 1) / 2
+    P = (2 * math.pi / 3) * rho * rc ** 3
+    return 9 * C + 30 * P, C, P
+
+
+ALG_BYTES_PER_ATOM_STEP = 216.0  # each FP64 state vector read once and written once
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=__import__("torch").device("cuda", local))
+    return ws, rank, local
+
+
+def barrier(ws):
+    import torch
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def reduce_max(ws, x):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline(replicas, steps, warm=1):
+    """The CPU oracle (reference algorithm, -O3 -ffast-math), one system per thread."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import ljref
+    sec = ljref.bench(N_ATOMS, WORK["T"], WORK["rho"], WORK["seed"], WORK["rc"], WORK["dt"], warm, steps,
+                      replicas, fast=True)
+    return replicas * N_ATOMS * steps / sec, sec
+
+
+def cpu_model():
+    try:
+        for l in open("/proc/cpuinfo"):
+            if l.startswith("model name"):
+                return l.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_reference(args, ws, rank):
+    """--impl reference: the reference's algorithm on the host cores (the CPU oracle
+    built with the reference's release flags; the reference itself needs Eigen and
+    Boost, which this image lacks).  Rank 0 only."""
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import ljref
+    cores = ljref.cpu_count()
+    replicas = max(1, min(cores, 64))
+    steps = max(1, min(args.steps, 8))
+    warm = max(1, min(args.warmup, 2))
+    value, sec = cpu_baseline(replicas, steps, warm)
+    sample = (f"{replicas} concurrent 1M-atom systems (one per thread, SimulationPool-style), "
+              f"{warm} warm-up + {steps} timed steps each; CPU: {cpu_model()}")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": steps, "warmup": warm, "ms_per_step": 1e3 * sec / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config({"implementation": "CPU oracle restatement of the reference, "
+                                                         "g++ -O3 -march=x86-64-v3 -ffast-math"}),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": replicas, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def timed_steps(torch, g, K, ws):
+    """K steps on the engine's stream bracketed by CUDA events (barrier + sync on both sides)."""
+    stream = torch.cuda.ExternalStream(g.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(ws)
+    e0.record(stream)
+    g.step_async(K)
+    e1.record(stream)
+    g.synchronize()
+    barrier(ws)
+    return e0.elapsed_time(e1) / 1e3
+
+
+def energy_drift(g, steps):
+    th = g.step(steps)
+    te = th[:, 3]
+    w = max(1, min(100, steps // 10))
+    return {"steps": steps, "abs_rel_drift": abs(te[-w:].mean() - te[:w].mean()) / abs(te[:w].mean()),
+            "max_rel_excursion": float(abs(te - te[0]).max() / abs(te[0]))}
+
+
+def e2e_run(torch, g, x, v, K):
+    """Public C-ABI path from pinned host buffers, copies inside the timed region."""
+    from lennardjonesium import _native as nat
+    N = g.N
+    pin = [torch.zeros((N, 4), dtype=torch.float64, pin_memory=True) for _ in range(8)]
+    pin[0][:, :3] = torch.from_numpy(x[:, :3])
+    pin[1][:, :3] = torch.from_numpy(v[:, :3])
+    rec = torch.zeros((K, 7), dtype=torch.float64, pin_memory=True)
+    P = lambda t: ctypes.c_void_p(t.data_ptr())
+    L = nat.lib()
+    stream = torch.cuda.ExternalStream(g.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    nat.check(L.lj_gpu_upload_state(g._ctx, P(pin[0]), P(pin[1]), P(pin[2]), P(pin[3]), 4, 0.0, 0.0, 0.0), g._ctx)
+    nat.check(L.lj_gpu_step(g._ctx, K, P(rec)), g._ctx)
+    t, pe, w = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    nat.check(L.lj_gpu_download_state(g._ctx, P(pin[4]), P(pin[5]), P(pin[6]), P(pin[7]), 4, ctypes.byref(t),
+                                      ctypes.byref(pe), ctypes.byref(w)), g._ctx)
+    e1.record(stream)
+    e1.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3
+    state_bytes = 4 * 32 * N
+    return {"value": N * K / sec, "unit": UNIT, "h2d_bytes_per_step": state_bytes / K,
+            "d2h_bytes_per_step": (state_bytes + 56 * K) / K,
+            "path": "lj_gpu_upload_state + lj_gpu_step(K, records to host) + lj_gpu_download_state, "
+                    "pinned host SystemState (4 x N doubles per vector)"}
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    from lennardjonesium import GpuSystem, initial_condition
+    from lennardjonesium import _native as nat
+
+    torch.cuda.set_device(local)
+    x, v, L = initial_condition(N_ATOMS, WORK["T"], WORK["rho"], WORK["seed"] + rank)
+    peaks = measured_peaks()
+    f64 = ctypes.c_double()
+    f32 = ctypes.c_double()
+    nat.check(nat.lib().lj_gpu_fma_peaks(local, ctypes.byref(f64), ctypes.byref(f32)))
+    F_alg, C, P = alg_flops_per_atom_step(N_ATOMS, L, WORK["rc"], WORK["rho"])
+
+    results = {}
+    for prec in ("fp64", "mixed"):
+        g = GpuSystem(N_ATOMS, L, cutoff=WORK["rc"], dt=WORK["dt"], precision=prec, device=local)
+        g.upload(x, v=v)
+        g.step_async(args.warmup)
+        g.synchronize()
+        launches0 = g.stats()["kernel_launches"]
+        with ClockSampler(local) as clk:
+            sec = timed_steps(torch, g, args.steps, ws)
+        launches = g.stats()["kernel_launches"] - launches0
+        sec = reduce_max(ws, sec)
+        ph = g.step_timed(min(args.steps, 200))
+        st = g.stats()
+        results[prec] = dict(sec=sec, phases=ph, clocks=clk.summary(), launches=launches, stats=st, g=g)
+
+    # energy drift at equal length for both paths (fresh systems from the same state)
+    drift = {}
+    if args.drift_steps > 0:
+        for prec in ("fp64", "mixed"):
+            g = results[prec]["g"]
+            g.upload(x, v=v)
+            drift[prec] = energy_drift(g, args.drift_steps)
+
+    e2e = e2e_run(torch, results["fp64"]["g"], x, v, args.steps)
+
+    r64 = results["fp64"]
+    K = args.steps
+    value = ws * N_ATOMS * K / r64["sec"]
+    ph = r64["phases"]
+    t_force = ph["force_ms"] / ph["steps"] / 1e3
+    flops = F_alg * N_ATOMS
+    achieved = flops / t_force / 1e12
+    traffic = None
+    tfile = ROOT / "profiles" / "force_fp64_traffic.json"
+    if tfile.exists():
+        traffic = json.loads(tfile.read_text()).get("bytes_per_launch_full_size")
+    roofline = {"bound": "fp64", "achieved": achieved, "peak": f64.value, "unit": "TFLOP/s",
+                "frac": achieved / f64.value, "traffic": traffic,
+                "kernel": "force_fp64_kernel (pair force + second kick + partial sums)",
+                "peak_source": "measured: project DFMA microbenchmark on this GPU (lj_gpu_fma_peaks)",
+                "alg_flops_per_atom_step": F_alg, "candidates_per_atom": C, "pairs_per_atom": P,
+                "kernel_ms": t_force * 1e3,
+                "hbm_frac_of_measured": (ALG_BYTES_PER_ATOM_STEP * N_ATOMS / (r64["sec"] / K)) / 1e9
+                / peaks.get("hbm_gbs", 6650.0)}
+    rm = results["mixed"]
+    phm = rm["phases"]
+    t_force_m = phm["force_ms"] / phm["steps"] / 1e3
+    mixed = {"value": ws * N_ATOMS * K / rm["sec"], "unit": UNIT, "ms_per_step": 1e3 * rm["sec"] / K,
+             "speedup_vs_fp64": r64["sec"] / rm["sec"],
+             "roofline": {"bound": "fp32", "achieved": flops / t_force_m / 1e12, "peak": f32.value,
+                          "unit": "TFLOP/s", "frac": flops / t_force_m / 1e12 / f32.value,
+                          "kernel_ms": t_force_m * 1e3},
+             "phases_ms_per_step": {k: phm[k] / phm["steps"] for k in ("kick_drift_ms", "rebuild_ms", "force_ms",
+                                                                        "finalize_ms")}}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": args.warmup,
+            "ms_per_step": 1e3 * r64["sec"] / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config({"precision": "fp64 (drop-in); mixed reported under 'mixed'"}),
+            "clocks": r64["clocks"], "e2e": e2e, "gpu_launches": r64["launches"], "roofline": roofline,
+            "mixed": mixed, "drift": drift,
+            "phases_ms_per_step": {k: ph[k] / ph["steps"] for k in ("kick_drift_ms", "rebuild_ms", "force_ms",
+                                                                     "finalize_ms")},
+            "list_builds_per_step": ph["rebuilds"] / ph["steps"],
+            "fma_peaks_tflops": {"fp64": f64.value, "fp32": f32.value}}
+    if ws == 1 and rank == 0 and not args.no_cpu_baseline:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import ljref
+        cores = max(1, min(ljref.cpu_count(), 64))
+        cval, csec = cpu_baseline(cores, 2, 1)
+        line["cpu_baseline"] = {"value": cval, "unit": UNIT, "cores": cores, "kind": "port",
+                                "sample": f"{cores} concurrent 1M-atom systems, one per thread, 1 warm-up + 2 "
+                                          f"timed steps each (CPU oracle, reference release flags); CPU: {cpu_model()}"}
+    for r in results.values():
+        r["g"].close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--drift-steps", type=int, default=10000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cells", type=int, default=64,
+                    help="FCC cells per box edge (N = 4 cells^3); 64 is the benchmark workload")
+    args = ap.parse_args()
+    global N_ATOMS
+    WORK["n_cells"] = args.cells
+    N_ATOMS = 4 * args.cells ** 3
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        # CPU only: rank 0 runs the reference arm, the other ranks exit at once
+        run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
+        return
+    ws, rank, local = dist_setup(args)
+    try:
+        run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

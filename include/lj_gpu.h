@@ -1,0 +1,204 @@
+/*
+ * lj_gpu.h -- C ABI of the B200 engine for lennard-jonesium's NVE hot path.
+ *
+ * Every entry point is plain C: opaque context pointer, plain pointers and
+ * sizes, int status codes.  All host arrays are borrowed for the duration of
+ * the call only.  A context owns its device buffers and one CUDA stream; use
+ * one context per host thread (the reference runs one simulation per thread,
+ * src/cpp/lennardjonesium/api/simulation_pool.cpp:35-42).  No entry point keeps
+ * global mutable state except where a comment says otherwise.
+ *
+ * Per-atom host arrays use the reference's SystemState layout when stride is 4:
+ * Eigen::Matrix4Xd column-major, (x0, y0, z0, w0, x1, ...), with w ignored on
+ * input and written as 0 on output (physics/system_state.hpp:85-95).  stride 3
+ * packs (x, y, z) per atom.
+ *
+ * Reference interfaces replaced (paths relative to the reference checkout):
+ *   engine::Integrator / VelocityVerletIntegrator::operator()
+ *       src/cpp/lennardjonesium/engine/integrator.hpp:34-102, integrator.cpp:62-88
+ *   engine::ShortRangeForceCalculation::operator()
+ *       src/cpp/lennardjonesium/engine/force_calculation.hpp:63-79, force_calculation.cpp:46-71
+ *   engine::CellListParticlePairFilter::pairs
+ *       src/cpp/lennardjonesium/engine/particle_pair_filter.cpp:132-192
+ *   engine::PeriodicBoundaryCondition::operator()
+ *       src/cpp/lennardjonesium/engine/boundary_condition.cpp:37-50
+ *   physics::LennardJonesForce::compute
+ *       src/cpp/lennardjonesium/physics/lennard_jones_force.cpp:76-128
+ *   physics::ThermodynamicMeasurement::operator()
+ *       src/cpp/lennardjonesium/physics/measurements.hpp:59-70
+ *   physics::set_temperature
+ *       src/cpp/lennardjonesium/physics/transformations.cpp:94-116
+ */
+#ifndef LJ_GPU_H
+#define LJ_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference reports misuse through assert() only
+ * (e.g. force_calculation.cpp:43, particle_pair_filter.cpp:61-64,
+ * lennard_jones_force.cpp:45); here each of those conditions returns LJ_ERR_ARG. */
+#define LJ_OK 0
+#define LJ_ERR_ARG 1        /* invalid argument (bad size, box below cutoff, null pointer) */
+#define LJ_ERR_CUDA 2       /* a CUDA call failed; lj_gpu_last_error() has the message */
+#define LJ_ERR_NONFINITE 3  /* a non-finite energy or virial appeared during a step */
+#define LJ_ERR_TIMEOUT 4    /* a bounded device-side wait gave up */
+#define LJ_ERR_CAPACITY 5   /* a neighbour list overflowed its capacity; results are invalid */
+
+/* Arithmetic of the pair kernel. */
+#define LJ_PRECISION_FP64 0   /* the drop-in: FP64 throughout */
+#define LJ_PRECISION_MIXED 1  /* FP32 pair arithmetic; FP64 accumulation, integration, sums */
+
+/* Pair force.  LJ is physics::LennardJonesForce (quadratic-spline truncation,
+ * eps = sigma = 1).  CONSTANT is the reference's test mock
+ * tests/cpp/mock/constant_short_range_force.cpp:31-59 (used for its known
+ * answers).  NONE means the integrator carries no force calculation, as an
+ * Integrator built without a ShortRangeForce (integrator.cpp:78-79). */
+#define LJ_FORCE_NONE 0
+#define LJ_FORCE_LJ 1
+#define LJ_FORCE_CONSTANT 2
+
+typedef struct lj_params {
+    int particle_count;      /* N >= 1 */
+    double box[3];           /* periodic box edge lengths (tools::BoundingBox) */
+    double cutoff_distance;  /* rc; each box edge must be >= rc (particle_pair_filter.cpp:61-64) */
+    double time_delta;       /* dt */
+    int precision;           /* LJ_PRECISION_* */
+    int force_kind;          /* LJ_FORCE_* */
+    double force_strength;   /* LJ_FORCE_CONSTANT only */
+    int periodic;            /* 1: PeriodicBoundaryCondition each step; 0: none (LJ_FORCE_NONE only) */
+    int device;              /* CUDA device ordinal */
+    double skin;             /* Verlet-list skin; < 0 selects the default (0.3) */
+    int neighbor_capacity;   /* list entries per atom; 0 selects a density-based default */
+} lj_params;
+
+/* One ThermodynamicMeasurement::Result (physics/measurements.hpp:42-56). */
+typedef struct lj_thermo {
+    double time;
+    double kinetic_energy;
+    double potential_energy;
+    double total_energy;
+    double virial;
+    double temperature;
+    double mean_square_displacement;
+} lj_thermo;
+
+/* Counters describing the work done so far (for tests and tuning). */
+typedef struct lj_stats {
+    long long steps;           /* velocity-Verlet steps taken */
+    long long list_builds;     /* neighbour-list rebuilds (cell binning + list) */
+    int neighbor_capacity;     /* list entries per atom */
+    int list_cells[3];         /* cell grid used for list builds */
+    int max_neighbors;         /* largest list seen at the last build */
+    int small_box;             /* 1: explicit lattice images, rebuilt every step */
+    double skin;               /* skin in use (0 in small-box mode) */
+    long long kernel_launches; /* kernels this context has launched */
+} lj_stats;
+
+typedef struct lj_ctx lj_ctx;
+
+/* Fill *p with the defaults of the reference's Configuration
+ * (api/configuration.hpp: rc 2.5, dt 0.005) plus FP64, LJ, periodic, device 0. */
+void lj_gpu_default_params(lj_params* p);
+
+/* Create a context with zeroed state (SystemState(N), system_state.cpp:29-37). */
+int lj_gpu_create(const lj_params* params, lj_ctx** out);
+int lj_gpu_destroy(lj_ctx* ctx);
+
+/* Last error message of this context (static storage owned by the context). */
+const char* lj_gpu_last_error(const lj_ctx* ctx);
+const char* lj_gpu_status_string(int status);
+
+/* Replace the whole state.  x, v, disp, F: N atoms each at `stride` doubles
+ * (3 or 4); any of v, disp, F may be NULL for zeros.  time, pe, virial are the
+ * SystemState scalars. */
+int lj_gpu_upload_state(lj_ctx* ctx, const double* x, const double* v, const double* disp,
+                        const double* F, int stride, double time, double pe, double virial);
+
+/* Copy the state out in atom-id order; NULL outputs are skipped. */
+int lj_gpu_download_state(lj_ctx* ctx, double* x, double* v, double* disp, double* F, int stride,
+                          double* time, double* pe, double* virial);
+
+/* ShortRangeForceCalculation::operator(): clear F, PE, W and recompute them
+ * from the current positions.  pe, virial may be NULL. */
+int lj_gpu_compute_forces(lj_ctx* ctx, double* pe, double* virial);
+
+/* Integrator::operator()(nsteps) followed, after every step, by a
+ * ThermodynamicMeasurement: out (may be NULL) receives nsteps records. */
+int lj_gpu_step(lj_ctx* ctx, int nsteps, lj_thermo* out);
+
+/* Instantaneous ThermodynamicMeasurement of the current state. */
+int lj_gpu_measure(lj_ctx* ctx, lj_thermo* out);
+
+/* Multiply every velocity by factor. */
+int lj_gpu_scale_velocities(lj_ctx* ctx, double factor);
+
+/* physics::set_temperature(target): v *= sqrt(target / T) with T measured from
+ * the current velocities; *measured (may be NULL) receives that T. */
+int lj_gpu_set_temperature(lj_ctx* ctx, double target, double* measured);
+
+/* The reference's cell binning of the current positions, for bit-exact checks
+ * (particle_pair_filter.cpp:141-154, cell_list_array.cpp:34-52):
+ *   shape[3]        floor(L / rc) per axis
+ *   cell_of[N]      flat cell index (x-major) of each atom id
+ *   offsets[nc+1]   exclusive prefix of the per-cell counts
+ *   members[N]      atom ids, cell-major, ascending within each cell
+ * Any output may be NULL; offsets needs shape[0]*shape[1]*shape[2]+1 ints
+ * (call once with offsets NULL to learn the shape). */
+int lj_gpu_debug_cells(lj_ctx* ctx, int* shape, int* cell_of, int* offsets, int* members);
+
+/* The pair set the force kernel used for the current positions: every
+ * unordered pair within the cutoff once, as (i < j by atom id, image code,
+ * r^2) with image code 9*(ix+1)+3*(iy+1)+(iz+1) and separation
+ * (x_i - x_j) - image * L.  Writes at most cap entries (in no particular
+ * order) and returns the total count, or a negative status. */
+long long lj_gpu_debug_pairs(lj_ctx* ctx, long long cap, int* i, int* j, int* image, double* r2);
+
+/* Radial distribution histogram of the current positions: ordered pairs
+ * (i != j) at minimum-image distance r < rmax in bin floor(r * nbins / rmax).
+ * rmax must be <= min(L) / 2.  hist receives nbins counts.  (New: the reference
+ * has no RDF.) */
+int lj_gpu_rdf(lj_ctx* ctx, int nbins, double rmax, unsigned long long* hist);
+
+int lj_gpu_get_stats(const lj_ctx* ctx, lj_stats* out);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that time or order
+ * work against it (e.g. torch.cuda.ExternalStream). */
+void* lj_gpu_stream(lj_ctx* ctx);
+
+/* Enqueue nsteps steps without waiting and without copying records back (the
+ * per-step records stay in the device ring).  lj_gpu_synchronize() waits and
+ * reports any capacity or non-finite error raised meanwhile. */
+int lj_gpu_step_async(lj_ctx* ctx, int nsteps);
+int lj_gpu_synchronize(lj_ctx* ctx);
+
+/* Device time of each phase of the step, accumulated over nsteps real steps
+ * with CUDA events recorded between the phases on the context's stream. */
+typedef struct lj_phase_times {
+    double kick_drift_ms;  /* first half kick, drift, wrap, displacement check */
+    double rebuild_ms;     /* cell binning + neighbour list (mostly gated off) */
+    double force_ms;       /* pair force + second kick + partial sums */
+    double finalize_ms;    /* fixed-order reduction and record */
+    long long steps;
+    long long rebuilds;
+} lj_phase_times;
+int lj_gpu_step_timed(lj_ctx* ctx, int nsteps, lj_phase_times* out);
+
+/* Measured FMA throughput of the CUDA-core FP64 and FP32 pipes of a device
+ * (TFLOP/s, 2 flops per FMA): the roofline denominators of the pair kernels. */
+int lj_gpu_fma_peaks(int device, double* fp64_tflops, double* fp32_tflops);
+
+/* engine::InitialCondition (engine/initial_condition.cpp:49-104,
+ * tools/cubic_lattice.cpp:38-86): FCC positions and libstdc++-seeded
+ * Maxwell-Boltzmann velocities with zero momentum and angular momentum,
+ * rescaled to T.  Host only (no GPU needed).  x, v: N x 4 doubles;
+ * *side receives the cubic box edge. */
+int lj_initial_condition(int N, double temperature, double density, unsigned seed, double* x, double* v,
+                         double* side);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LJ_GPU_H */

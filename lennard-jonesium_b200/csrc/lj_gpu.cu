@@ -1,0 +1,778 @@
+// lj_gpu.cu -- host side of the C ABI declared in include/lj_gpu.h.
+//
+// One context = one system on one device, driven on the context's own stream.
+// A velocity-Verlet step (integrator.cpp:62-88) is the launch sequence
+//   kick_drift -> [rebuild chain] -> force (+ second kick + partial sums) -> finalize
+// where the rebuild chain (cell binning by counting sort, neighbour list) is
+// launched every step but returns at once unless the device-side skin
+// criterion (max displacement since the last build > skin / 2) or the host
+// asked for a rebuild.  Per-step records land in a device ring and are copied
+// to the host once per lj_gpu_step call.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/lj_gpu.h"
+#include "lj_kernels.cuh"
+#include "lj_mixed.cuh"
+
+using namespace ljb;
+
+struct lj_ctx {
+    lj_params p{};
+    int N = 0;
+    PairParams pp{};
+    double skin = 0.0;
+    bool small_box = false;
+    bool rebuild_always = false;
+    Grid list_grid{};
+    Grid ref_grid{};
+    int cap = 0;
+    int nblocks = 0;
+    cudaStream_t stream = nullptr;
+
+    // device buffers
+    double4* pos = nullptr;
+    double4* pos_tmp = nullptr;
+    double* soa = nullptr;
+    double* soa_tmp = nullptr;
+    double* bd = nullptr;
+    int* ids = nullptr;
+    int* ids_tmp = nullptr;
+    int* cell_of = nullptr;
+    int* rank = nullptr;
+    int* order = nullptr;
+    int* count = nullptr;
+    int* start = nullptr;
+    int* tile_sums = nullptr;
+    uint4* nbr = nullptr;        // neighbour list, groups of 4 entries
+    float4* posf = nullptr;      // FP32 copy of the sorted positions (list builds)
+    int* cnt = nullptr;
+    double* partials = nullptr;
+    Scalars* sc = nullptr;
+    double* ring = nullptr;     // ring_cap records of 7 doubles
+    double* dscratch = nullptr; // small device scratch (set_temperature factor, L)
+    double* dL = nullptr;
+    int ring_cap = 0;
+    double* host_ring = nullptr;  // pinned
+
+    // mixed-precision buffers
+    float4* posl = nullptr;
+    double* bx = nullptr;  // x at build (unwrapped reference for local coordinates)
+
+    // debug (reference grid) buffers, allocated on first use
+    int* dbg_count = nullptr;
+    int* dbg_start = nullptr;
+    int* dbg_members = nullptr;
+    int* dbg_cell_of = nullptr;
+    int* dbg_tiles = nullptr;
+
+    long long launches = 0;
+    char err[512] = {0};
+};
+
+namespace {
+
+const char* kStatus[] = {"ok", "invalid argument", "CUDA error", "non-finite energy or virial",
+                         "device wait timed out", "neighbour list capacity exceeded"};
+
+int set_err(lj_ctx* c, int code, const char* msg) {
+    if (c) std::snprintf(c->err, sizeof c->err, "%s", msg);
+    return code;
+}
+
+#define CK(call)                                                                       \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess) {                                                       \
+            if (ctx) std::snprintf(ctx->err, sizeof ctx->err, "%s: %s (%s:%d)", #call, \
+                                   cudaGetErrorString(e_), __FILE__, __LINE__);        \
+            return LJ_ERR_CUDA;                                                        \
+        }                                                                              \
+    } while (0)
+
+#define CKL()                                                                           \
+    do {                                                                                \
+        ++ctx->launches;                                                                \
+        cudaError_t e_ = cudaGetLastError();                                            \
+        if (e_ != cudaSuccess) {                                                        \
+            std::snprintf(ctx->err, sizeof ctx->err, "launch: %s (%s:%d)",              \
+                          cudaGetErrorString(e_), __FILE__, __LINE__);                  \
+            return LJ_ERR_CUDA;                                                         \
+        }                                                                               \
+    } while (0)
+
+int blocks_for(int n, int t = kThreads) { return (n + t - 1) / t; }
+
+Grid make_grid(const double L[3], double cell_min) {
+    Grid g;
+    for (int k = 0; k < 3; ++k) {
+        g.n[k] = std::max(1, (int)std::floor(L[k] / cell_min));
+        g.ratio[k] = (double)g.n[k] / L[k];
+    }
+    return g;
+}
+
+int hiword(double x) {
+    long long b;
+    std::memcpy(&b, &x, 8);
+    return (int)(b >> 32);
+}
+
+Gate gate_of(lj_ctx* c) {
+    Gate g;
+    g.sc = c->sc;
+    double h = 0.5 * c->skin;
+    g.thresh2 = h * h * 0.999;
+    g.always = c->rebuild_always ? 1 : 0;
+    return g;
+}
+
+Soa soa_of(double* p, int N) { return Soa{p, N}; }
+
+// Counting sort of atoms into grid g (histogram, scan, scatter); rank/cell_of per slot.
+template <bool GATED>
+int launch_binning(lj_ctx* ctx, const Grid& g, int* count, int* start, int* tiles, Gate gate) {
+    int nc = g.ncell();
+    int ntiles = (nc + kScanTile - 1) / kScanTile;
+    bin_count_kernel<GATED><<<blocks_for(ctx->N), kThreads, 0, ctx->stream>>>(
+        ctx->N, ctx->pos, g, ctx->cell_of, ctx->rank, count, gate);
+    CKL();
+    scan_reduce_kernel<GATED><<<ntiles, 1024, 0, ctx->stream>>>(count, nc, tiles, gate);
+    CKL();
+    scan_tiles_kernel<GATED><<<1, 1024, 0, ctx->stream>>>(tiles, ntiles, gate);
+    CKL();
+    scan_apply_kernel<GATED><<<ntiles, 1024, 0, ctx->stream>>>(count, nc, tiles, start, gate);
+    CKL();
+    return LJ_OK;
+}
+
+// Rebuild chain: bin into the list grid, sort, gather, list.  Every kernel
+// returns at once when the gate is closed.
+int launch_rebuild(lj_ctx* ctx) {
+    Gate gate = gate_of(ctx);
+    int N = ctx->N;
+    int rc = launch_binning<true>(ctx, ctx->list_grid, ctx->count, ctx->start, ctx->tile_sums, gate);
+    if (rc) return rc;
+    scatter_kernel<true><<<blocks_for(N), kThreads, 0, ctx->stream>>>(N, ctx->cell_of, ctx->rank,
+                                                                        ctx->start, ctx->order, gate);
+    CKL();
+    cell_sort_kernel<true><<<blocks_for(ctx->list_grid.ncell()), kThreads, 0, ctx->stream>>>(
+        ctx->list_grid.ncell(), ctx->start, ctx->order, gate);
+    CKL();
+    gather_kernel<<<blocks_for(N), kThreads, 0, ctx->stream>>>(
+        N, ctx->order, ctx->pos, ctx->pos_tmp, soa_of(ctx->soa, N), soa_of(ctx->soa_tmp, N), ctx->ids,
+        ctx->ids_tmp, ctx->bd, gate);
+    CKL();
+    copy_back_kernel<<<blocks_for(N), kThreads, 0, ctx->stream>>>(
+        N, ctx->pos_tmp, ctx->pos, soa_of(ctx->soa_tmp, N), soa_of(ctx->soa, N), ctx->ids_tmp, ctx->ids,
+        ctx->posf, gate);
+    CKL();
+    // FP32 candidate radius, widened past FP32 rounding of box coordinates so the
+    // list is a superset of the FP64 pair set
+    double Lmax = std::max(ctx->pp.L[0], std::max(ctx->pp.L[1], ctx->pp.L[2]));
+    double cut = ctx->pp.rc + ctx->skin + 8.0 * Lmax * std::ldexp(1.0, -24) + 1e-6;
+    float cut2 = (float)(cut * cut);
+    float3 Lf = make_float3((float)ctx->pp.L[0], (float)ctx->pp.L[1], (float)ctx->pp.L[2]);
+    if (ctx->small_box)
+        build_list_kernel<true><<<blocks_for(N), kThreads, 0, ctx->stream>>>(
+            N, ctx->pos, ctx->posf, ctx->list_grid, ctx->start, Lf, cut2, ctx->cap, ctx->nbr, ctx->cnt, ctx->sc, gate);
+    else
+        build_list_kernel<false><<<blocks_for(N), kThreads, 0, ctx->stream>>>(
+            N, ctx->pos, ctx->posf, ctx->list_grid, ctx->start, Lf, cut2, ctx->cap, ctx->nbr, ctx->cnt, ctx->sc, gate);
+    CKL();
+    if (ctx->p.precision == LJ_PRECISION_MIXED) {
+        mixed_build_local_kernel<<<blocks_for(N), kThreads, 0, ctx->stream>>>(
+            N, ctx->pos, soa_of(ctx->soa, N), ctx->list_grid, ctx->bx, ctx->posl, gate);
+        CKL();
+    }
+    return LJ_OK;
+}
+
+int launch_force(lj_ctx* ctx, bool kick) {
+    int N = ctx->N;
+    Soa s = soa_of(ctx->soa, N);
+    dim3 gr(ctx->nblocks), bl(kThreads);
+    int kind = ctx->p.force_kind;
+    if (ctx->p.precision == LJ_PRECISION_MIXED && kind == LJ_FORCE_LJ && !ctx->small_box) {
+        if (kick)
+            force_mixed_kernel<true><<<gr, bl, 0, ctx->stream>>>(N, ctx->posl, s, ctx->nbr, ctx->cnt,
+                                                                  ctx->pp, mixed_params(ctx->pp, ctx->list_grid),
+                                                                  ctx->partials);
+        else
+            force_mixed_kernel<false><<<gr, bl, 0, ctx->stream>>>(N, ctx->posl, s, ctx->nbr, ctx->cnt,
+                                                                   ctx->pp, mixed_params(ctx->pp, ctx->list_grid),
+                                                                   ctx->partials);
+        CKL();
+        return LJ_OK;
+    }
+#define LJ_FORCE_LAUNCH(K, S, KK)                                                                \
+    force_fp64_kernel<K, S, KK><<<gr, bl, 0, ctx->stream>>>(N, ctx->pos, s, ctx->nbr, ctx->cnt, \
+                                                            ctx->pp, ctx->partials)
+    bool sm = ctx->small_box;
+    if (kind == LJ_FORCE_LJ) {
+        if (sm) { if (kick) LJ_FORCE_LAUNCH(KIND_LJ, true, true); else LJ_FORCE_LAUNCH(KIND_LJ, true, false); }
+        else { if (kick) LJ_FORCE_LAUNCH(KIND_LJ, false, true); else LJ_FORCE_LAUNCH(KIND_LJ, false, false); }
+    } else {
+        if (sm) { if (kick) LJ_FORCE_LAUNCH(KIND_CONST, true, true); else LJ_FORCE_LAUNCH(KIND_CONST, true, false); }
+        else { if (kick) LJ_FORCE_LAUNCH(KIND_CONST, false, true); else LJ_FORCE_LAUNCH(KIND_CONST, false, false); }
+    }
+#undef LJ_FORCE_LAUNCH
+    CKL();
+    return LJ_OK;
+}
+
+int launch_kick_drift(lj_ctx* ctx) {
+    int N = ctx->N;
+    bool track = !ctx->rebuild_always && ctx->p.force_kind != LJ_FORCE_NONE;
+    Soa s = soa_of(ctx->soa, N);
+    dim3 gr(ctx->nblocks), bl(kThreads);
+    if (ctx->p.periodic) {
+        if (track) kick_drift_kernel<true, true><<<gr, bl, 0, ctx->stream>>>(N, ctx->pos, s, ctx->bd, ctx->pp, ctx->sc);
+        else kick_drift_kernel<true, false><<<gr, bl, 0, ctx->stream>>>(N, ctx->pos, s, ctx->bd, ctx->pp, ctx->sc);
+    } else {
+        kick_drift_kernel<false, false><<<gr, bl, 0, ctx->stream>>>(N, ctx->pos, s, ctx->bd, ctx->pp, ctx->sc);
+    }
+    CKL();
+    if (ctx->p.precision == LJ_PRECISION_MIXED && ctx->p.force_kind == LJ_FORCE_LJ && !ctx->small_box) {
+        mixed_update_local_kernel<<<gr, bl, 0, ctx->stream>>>(N, s, ctx->bd, ctx->bx, ctx->list_grid,
+                                                              ctx->posl);
+        CKL();
+    }
+    return LJ_OK;
+}
+
+// One velocity-Verlet step writing its record to ring slot `slot`.
+int launch_step(lj_ctx* ctx, int slot) {
+    int rc = launch_kick_drift(ctx);
+    if (rc) return rc;
+    bool forces = ctx->p.force_kind != LJ_FORCE_NONE;
+    if (forces) {
+        rc = launch_rebuild(ctx);
+        if (rc) return rc;
+        rc = launch_force(ctx, true);
+        if (rc) return rc;
+    } else {
+        kick_measure_kernel<<<ctx->nblocks, kThreads, 0, ctx->stream>>>(ctx->N, soa_of(ctx->soa, ctx->N),
+                                                                         ctx->pp.dt, 1, ctx->partials);
+        CKL();
+    }
+    finalize_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->partials, ctx->nblocks, ctx->N, ctx->pp.dt, 0,
+                                                 forces ? 1 : 0, ctx->sc, ctx->ring + 7 * (size_t)slot);
+    CKL();
+    return LJ_OK;
+}
+
+int read_flags(lj_ctx* ctx) {
+    Scalars h;
+    CK(cudaMemcpyAsync(&h, ctx->sc, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (h.overflow) return set_err(ctx, LJ_ERR_CAPACITY, "neighbour list capacity exceeded");
+    if (h.nonfinite) return set_err(ctx, LJ_ERR_NONFINITE, "non-finite energy or virial");
+    return LJ_OK;
+}
+
+void free_all(lj_ctx* c) {
+    void* ptrs[] = {c->posf, c->pos, c->pos_tmp, c->soa, c->soa_tmp, c->bd, c->ids, c->ids_tmp, c->cell_of,
+                    c->rank, c->order, c->count, c->start, c->tile_sums, c->nbr, c->cnt, c->partials,
+                    c->sc, c->ring, c->dscratch, c->posl, c->bx, c->dbg_count, c->dbg_start,
+                    c->dbg_members, c->dbg_cell_of, c->dbg_tiles};
+    for (void* q : ptrs)
+        if (q) cudaFree(q);
+    if (c->host_ring) cudaFreeHost(c->host_ring);
+    if (c->stream) cudaStreamDestroy(c->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+void lj_gpu_default_params(lj_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof *p);
+    p->particle_count = 0;
+    p->box[0] = p->box[1] = p->box[2] = 1.0;
+    p->cutoff_distance = 2.5;
+    p->time_delta = 0.005;
+    p->precision = LJ_PRECISION_FP64;
+    p->force_kind = LJ_FORCE_LJ;
+    p->force_strength = 0.0;
+    p->periodic = 1;
+    p->device = 0;
+    p->skin = -1.0;
+    p->neighbor_capacity = 0;
+}
+
+const char* lj_gpu_status_string(int s) {
+    return (s >= 0 && s <= 5) ? kStatus[s] : "unknown status";
+}
+
+const char* lj_gpu_last_error(const lj_ctx* ctx) { return ctx ? ctx->err : "null context"; }
+
+int lj_gpu_create(const lj_params* params, lj_ctx** out) {
+    lj_ctx* ctx = nullptr;
+    if (!params || !out) return LJ_ERR_ARG;
+    *out = nullptr;
+    const lj_params& p = *params;
+    if (p.particle_count < 1 || p.particle_count >= kMaxAtoms) return LJ_ERR_ARG;
+    if (!(p.cutoff_distance > 0) || !(p.time_delta >= 0)) return LJ_ERR_ARG;
+    for (int k = 0; k < 3; ++k) {
+        if (!(p.box[k] > 0) || !std::isfinite(p.box[k])) return LJ_ERR_ARG;
+        // particle_pair_filter.cpp:61-64 -- only a pair filter needs box >= rc
+        if (p.force_kind != LJ_FORCE_NONE && !(p.box[k] >= p.cutoff_distance)) return LJ_ERR_ARG;
+    }
+    if (p.force_kind < LJ_FORCE_NONE || p.force_kind > LJ_FORCE_CONSTANT) return LJ_ERR_ARG;
+    if (p.precision != LJ_PRECISION_FP64 && p.precision != LJ_PRECISION_MIXED) return LJ_ERR_ARG;
+    if (!p.periodic && p.force_kind != LJ_FORCE_NONE) return LJ_ERR_ARG;
+    // lennard_jones_force.cpp:45 -- the cutoff must lie beyond the potential minimum
+    if (p.force_kind == LJ_FORCE_LJ && !(p.cutoff_distance * p.cutoff_distance > std::cbrt(2.0)))
+        return LJ_ERR_ARG;
+
+    ctx = new (std::nothrow) lj_ctx();
+    if (!ctx) return LJ_ERR_ARG;
+    ctx->p = p;
+    int N = ctx->N = p.particle_count;
+    CK(cudaSetDevice(p.device));
+    CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+
+    // pair constants (lennard_jones_force.cpp:33-74)
+    PairParams& pp = ctx->pp;
+    double rc = p.cutoff_distance;
+    pp.rc = rc;
+    pp.rc2 = rc * rc;
+    pp.inv_rc2 = 1.0 / pp.rc2;
+    double rcm6 = 1 / (pp.rc2 * pp.rc2 * pp.rc2);
+    pp.alpha = -4.0 * rcm6 * (rcm6 - 1.0);
+    pp.beta = 12.0 * rcm6 * (2.0 * rcm6 - 1.0);
+    pp.strength = p.force_strength;
+    pp.dt = p.time_delta;
+    double near = rc * (1.0 + 1e-9);
+    pp.near_lo = near;
+    for (int k = 0; k < 3; ++k) {
+        pp.L[k] = p.box[k];
+        pp.halfL[k] = 0.5 * p.box[k];
+        pp.halfL_hi[k] = hiword(0.5 * p.box[k]);
+        pp.near_hi[k] = p.box[k] - near;
+    }
+
+    // neighbour-list grid: cells of at least rc + skin, and >= 3 per axis for
+    // the minimum-image form; otherwise zero skin and a rebuild every step.
+    double skin = p.skin < 0 ? 0.3 : p.skin;
+    double Lmin = std::min(p.box[0], std::min(p.box[1], p.box[2]));
+    if (p.force_kind == LJ_FORCE_NONE || std::floor(Lmin / (rc + skin)) < 3) skin = 0.0;
+    ctx->skin = skin;
+    ctx->ref_grid = make_grid(p.box, rc);
+    ctx->list_grid = make_grid(p.box, rc + skin);
+    ctx->small_box = std::min(ctx->list_grid.n[0], std::min(ctx->list_grid.n[1], ctx->list_grid.n[2])) < 3;
+    ctx->rebuild_always = skin == 0.0;
+    if (ctx->list_grid.ncell() > kScanTile * kMaxScanTiles || ctx->ref_grid.ncell() > kScanTile * kMaxScanTiles) {
+        delete ctx;
+        return LJ_ERR_ARG;
+    }
+
+    double V = p.box[0] * p.box[1] * p.box[2];
+    double rho = N / V;
+    double cut = rc + skin;
+    double expect = 4.0 / 3.0 * M_PI * cut * cut * cut * std::max(rho, 1.2);
+    int cap = p.neighbor_capacity > 0 ? p.neighbor_capacity : (int)std::ceil(1.5 * expect + 32);
+    cap = std::min(cap, std::max(N - 1, 1) * 27);
+    cap = (std::max(cap, 1) + 3) & ~3;  // whole groups of 4
+    ctx->cap = cap;
+    ctx->nblocks = blocks_for(N);
+
+    int ncl = ctx->list_grid.ncell();
+    // slot N is a ghost far outside the box: it pads the last neighbour group
+    CK(cudaMalloc(&ctx->pos, sizeof(double4) * (N + 1)));
+    CK(cudaMalloc(&ctx->posf, sizeof(float4) * (N + 1)));
+    CK(cudaMalloc(&ctx->pos_tmp, sizeof(double4) * N));
+    CK(cudaMalloc(&ctx->soa, sizeof(double) * SOA_FIELDS * N));
+    CK(cudaMalloc(&ctx->soa_tmp, sizeof(double) * SOA_FIELDS * N));
+    CK(cudaMalloc(&ctx->bd, sizeof(double) * 3 * N));
+    CK(cudaMalloc(&ctx->ids, sizeof(int) * N));
+    CK(cudaMalloc(&ctx->ids_tmp, sizeof(int) * N));
+    CK(cudaMalloc(&ctx->cell_of, sizeof(int) * N));
+    CK(cudaMalloc(&ctx->rank, sizeof(int) * N));
+    CK(cudaMalloc(&ctx->order, sizeof(int) * N));
+    CK(cudaMalloc(&ctx->count, sizeof(int) * ncl));
+    CK(cudaMalloc(&ctx->start, sizeof(int) * (ncl + 1)));
+    CK(cudaMalloc(&ctx->tile_sums, sizeof(int) * kMaxScanTiles));
+    CK(cudaMalloc(&ctx->nbr, sizeof(uint4) * (size_t)(cap / 4) * N));
+    CK(cudaMalloc(&ctx->cnt, sizeof(int) * N));
+    CK(cudaMalloc(&ctx->partials, sizeof(double) * 4 * ctx->nblocks));
+    CK(cudaMalloc(&ctx->sc, sizeof(Scalars)));
+    ctx->ring_cap = 1024;
+    CK(cudaMalloc(&ctx->ring, sizeof(double) * 7 * ctx->ring_cap));
+    CK(cudaMalloc(&ctx->dscratch, sizeof(double) * 8));
+    ctx->dL = ctx->dscratch + 4;
+    CK(cudaMallocHost(&ctx->host_ring, sizeof(double) * 7 * ctx->ring_cap));
+    if (p.precision == LJ_PRECISION_MIXED) {
+        CK(cudaMalloc(&ctx->posl, sizeof(float4) * (N + 1)));
+        CK(cudaMalloc(&ctx->bx, sizeof(double) * 3 * N));
+        CK(cudaMemsetAsync(ctx->posl, 0, sizeof(float4) * N, ctx->stream));
+        float4 gl = make_float4(1e18f, 1e18f, 1e18f, 0.f);
+        CK(cudaMemcpyAsync(ctx->posl + N, &gl, sizeof gl, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemsetAsync(ctx->bx, 0, sizeof(double) * 3 * N, ctx->stream));
+    }
+    CK(cudaMemsetAsync(ctx->pos, 0, sizeof(double4) * N, ctx->stream));
+    CK(cudaMemsetAsync(ctx->posf, 0, sizeof(float4) * N, ctx->stream));
+    static const double4 ghost = make_double4(1e18, 1e18, 1e18, 0.0);
+    static const float4 ghostf = make_float4(1e18f, 1e18f, 1e18f, 0.f);
+    CK(cudaMemcpyAsync(ctx->pos + N, &ghost, sizeof ghost, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->posf + N, &ghostf, sizeof ghostf, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemsetAsync(ctx->soa, 0, sizeof(double) * SOA_FIELDS * N, ctx->stream));
+    CK(cudaMemsetAsync(ctx->bd, 0, sizeof(double) * 3 * N, ctx->stream));
+    CK(cudaMemsetAsync(ctx->count, 0, sizeof(int) * ncl, ctx->stream));
+    CK(cudaMemsetAsync(ctx->cnt, 0, sizeof(int) * N, ctx->stream));
+    CK(cudaMemsetAsync(ctx->sc, 0, sizeof(Scalars), ctx->stream));
+    CK(cudaMemcpyAsync(ctx->dL, p.box, sizeof(double) * 3, cudaMemcpyHostToDevice, ctx->stream));
+    // identity permutation
+    std::vector<int> ident(N);
+    for (int i = 0; i < N; ++i) ident[i] = i;
+    CK(cudaMemcpyAsync(ctx->ids, ident.data(), sizeof(int) * N, cudaMemcpyHostToDevice, ctx->stream));
+    int one = 1;
+    CK(cudaMemcpyAsync(&ctx->sc->need_rebuild, &one, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    *out = ctx;
+    return LJ_OK;
+}
+
+int lj_gpu_destroy(lj_ctx* ctx) {
+    if (!ctx) return LJ_ERR_ARG;
+    cudaSetDevice(ctx->p.device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    free_all(ctx);
+    delete ctx;
+    return LJ_OK;
+}
+
+int lj_gpu_upload_state(lj_ctx* ctx, const double* x, const double* v, const double* disp,
+                        const double* F, int stride, double time, double pe, double virial) {
+    if (!ctx || !x || (stride != 3 && stride != 4)) return set_err(ctx, LJ_ERR_ARG, "bad upload arguments");
+    CK(cudaSetDevice(ctx->p.device));
+    int N = ctx->N;
+    size_t bytes = sizeof(double) * (size_t)stride * N;
+    double* stage = reinterpret_cast<double*>(ctx->pos_tmp);  // 4N doubles of room
+    Soa s = soa_of(ctx->soa, N);
+    const double* src[4] = {x, v, disp, F};
+    int field[4] = {-1, VX, DX, FX};
+    for (int q = 0; q < 4; ++q) {
+        if (!src[q]) {
+            CK(cudaMemsetAsync(ctx->soa + (size_t)field[q] * N, 0, sizeof(double) * 3 * N, ctx->stream));
+            continue;
+        }
+        CK(cudaMemcpyAsync(stage, src[q], bytes, cudaMemcpyHostToDevice, ctx->stream));
+        unpack_kernel<<<blocks_for(N), kThreads, 0, ctx->stream>>>(N, stage, stride, field[q], ctx->pos, s,
+                                                                    ctx->ids);
+        CKL();
+    }
+    Scalars h{};
+    h.t = time;
+    h.pe = pe;
+    h.vir = virial;
+    h.need_rebuild = 1;
+    Scalars old;
+    CK(cudaMemcpyAsync(&old, ctx->sc, sizeof old, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    h.builds = old.builds;
+    h.steps = old.steps;
+    CK(cudaMemcpyAsync(ctx->sc, &h, sizeof h, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return LJ_OK;
+}
+
+int lj_gpu_download_state(lj_ctx* ctx, double* x, double* v, double* disp, double* F, int stride,
+                          double* time, double* pe, double* virial) {
+    if (!ctx || (stride != 3 && stride != 4)) return set_err(ctx, LJ_ERR_ARG, "bad download arguments");
+    CK(cudaSetDevice(ctx->p.device));
+    int N = ctx->N;
+    size_t bytes = sizeof(double) * (size_t)stride * N;
+    double* stage = reinterpret_cast<double*>(ctx->pos_tmp);
+    Soa s = soa_of(ctx->soa, N);
+    double* dst[4] = {x, v, disp, F};
+    int field[4] = {-1, VX, DX, FX};
+    for (int q = 0; q < 4; ++q) {
+        if (!dst[q]) continue;
+        pack_kernel<<<blocks_for(N), kThreads, 0, ctx->stream>>>(N, stage, stride, field[q], ctx->pos, s,
+                                                                  ctx->ids);
+        CKL();
+        CK(cudaMemcpyAsync(dst[q], stage, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    Scalars h;
+    CK(cudaMemcpyAsync(&h, ctx->sc, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (time) *time = h.t;
+    if (pe) *pe = h.pe;
+    if (virial) *virial = h.vir;
+    return LJ_OK;
+}
+
+int lj_gpu_compute_forces(lj_ctx* ctx, double* pe, double* virial) {
+    if (!ctx) return LJ_ERR_ARG;
+    CK(cudaSetDevice(ctx->p.device));
+    if (ctx->p.force_kind == LJ_FORCE_NONE) {
+        // no force calculation configured: clear_dynamics only
+        CK(cudaMemsetAsync(ctx->soa + (size_t)FX * ctx->N, 0, sizeof(double) * 3 * ctx->N, ctx->stream));
+        double z[3] = {0, 0, 0};
+        CK(cudaMemcpyAsync(&ctx->sc->pe, z, sizeof(double) * 2, cudaMemcpyHostToDevice, ctx->stream));
+    } else {
+        int one = 1;
+        CK(cudaMemcpyAsync(&ctx->sc->need_rebuild, &one, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        int rc = launch_rebuild(ctx);
+        if (rc) return rc;
+        rc = launch_force(ctx, false);
+        if (rc) return rc;
+        finalize_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->partials, ctx->nblocks, ctx->N, ctx->pp.dt, 1, 1,
+                                                     ctx->sc, ctx->ring);
+        CKL();
+    }
+    int rc = read_flags(ctx);
+    if (rc) return rc;
+    Scalars h;
+    CK(cudaMemcpyAsync(&h, ctx->sc, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (pe) *pe = h.pe;
+    if (virial) *virial = h.vir;
+    return LJ_OK;
+}
+
+int lj_gpu_step(lj_ctx* ctx, int nsteps, lj_thermo* out) {
+    if (!ctx || nsteps < 0) return set_err(ctx, LJ_ERR_ARG, "bad step arguments");
+    CK(cudaSetDevice(ctx->p.device));
+    int done = 0;
+    while (done < nsteps) {
+        int chunk = std::min(nsteps - done, ctx->ring_cap);
+        for (int s = 0; s < chunk; ++s) {
+            int rc = launch_step(ctx, s);
+            if (rc) return rc;
+        }
+        if (out) {
+            CK(cudaMemcpyAsync(ctx->host_ring, ctx->ring, sizeof(double) * 7 * chunk, cudaMemcpyDeviceToHost,
+                               ctx->stream));
+        }
+        int rc = read_flags(ctx);  // synchronises
+        if (rc) return rc;
+        if (out) std::memcpy(out + done, ctx->host_ring, sizeof(double) * 7 * chunk);
+        done += chunk;
+    }
+    return LJ_OK;
+}
+
+int lj_gpu_measure(lj_ctx* ctx, lj_thermo* out) {
+    if (!ctx || !out) return set_err(ctx, LJ_ERR_ARG, "bad measure arguments");
+    CK(cudaSetDevice(ctx->p.device));
+    kick_measure_kernel<<<ctx->nblocks, kThreads, 0, ctx->stream>>>(ctx->N, soa_of(ctx->soa, ctx->N), 0.0, 0,
+                                                                     ctx->partials);
+    CKL();
+    finalize_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->partials, ctx->nblocks, ctx->N, ctx->pp.dt, 2, 0,
+                                                 ctx->sc, ctx->ring);
+    CKL();
+    CK(cudaMemcpyAsync(ctx->host_ring, ctx->ring, sizeof(double) * 7, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    std::memcpy(out, ctx->host_ring, sizeof(double) * 7);
+    return LJ_OK;
+}
+
+int lj_gpu_scale_velocities(lj_ctx* ctx, double factor) {
+    if (!ctx || !std::isfinite(factor)) return set_err(ctx, LJ_ERR_ARG, "bad scale factor");
+    CK(cudaSetDevice(ctx->p.device));
+    scale_kernel<<<ctx->nblocks, kThreads, 0, ctx->stream>>>(ctx->N, soa_of(ctx->soa, ctx->N), factor);
+    CKL();
+    CK(cudaStreamSynchronize(ctx->stream));
+    return LJ_OK;
+}
+
+int lj_gpu_set_temperature(lj_ctx* ctx, double target, double* measured) {
+    if (!ctx || !(target >= 0)) return set_err(ctx, LJ_ERR_ARG, "bad target temperature");
+    lj_thermo m;
+    int rc = lj_gpu_measure(ctx, &m);
+    if (rc) return rc;
+    if (!(m.temperature > 0)) return set_err(ctx, LJ_ERR_ARG, "cannot scale a zero-temperature state");
+    if (measured) *measured = m.temperature;
+    return lj_gpu_scale_velocities(ctx, std::sqrt(target / m.temperature));
+}
+
+int lj_gpu_debug_cells(lj_ctx* ctx, int* shape, int* cell_of, int* offsets, int* members) {
+    if (!ctx) return LJ_ERR_ARG;
+    CK(cudaSetDevice(ctx->p.device));
+    const Grid& g = ctx->ref_grid;
+    if (shape)
+        for (int k = 0; k < 3; ++k) shape[k] = g.n[k];
+    if (!cell_of && !offsets && !members) return LJ_OK;
+    int nc = g.ncell(), N = ctx->N;
+    if (!ctx->dbg_count) {
+        CK(cudaMalloc(&ctx->dbg_count, sizeof(int) * nc));
+        CK(cudaMalloc(&ctx->dbg_start, sizeof(int) * (nc + 1)));
+        CK(cudaMalloc(&ctx->dbg_members, sizeof(int) * N));
+        CK(cudaMalloc(&ctx->dbg_cell_of, sizeof(int) * N));
+        CK(cudaMalloc(&ctx->dbg_tiles, sizeof(int) * kMaxScanTiles));
+        CK(cudaMemsetAsync(ctx->dbg_count, 0, sizeof(int) * nc, ctx->stream));
+    }
+    Gate open{};
+    open.sc = ctx->sc;
+    open.always = 1;
+    int rc = launch_binning<false>(ctx, g, ctx->dbg_count, ctx->dbg_start, ctx->dbg_tiles, open);
+    if (rc) return rc;
+    debug_members_kernel<<<blocks_for(N), kThreads, 0, ctx->stream>>>(N, ctx->cell_of, ctx->rank, ctx->dbg_start,
+                                                                       ctx->ids, ctx->dbg_members, ctx->dbg_cell_of);
+    CKL();
+    sort_members_kernel<<<blocks_for(nc), kThreads, 0, ctx->stream>>>(nc, ctx->dbg_start, ctx->dbg_members);
+    CKL();
+    if (cell_of) CK(cudaMemcpyAsync(cell_of, ctx->dbg_cell_of, sizeof(int) * N, cudaMemcpyDeviceToHost, ctx->stream));
+    if (offsets) CK(cudaMemcpyAsync(offsets, ctx->dbg_start, sizeof(int) * (nc + 1), cudaMemcpyDeviceToHost, ctx->stream));
+    if (members) CK(cudaMemcpyAsync(members, ctx->dbg_members, sizeof(int) * N, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    // the shared cell_of/rank scratch now holds the reference grid: force a list rebuild
+    int one = 1;
+    CK(cudaMemcpy(&ctx->sc->need_rebuild, &one, sizeof(int), cudaMemcpyHostToDevice));
+    return LJ_OK;
+}
+
+long long lj_gpu_debug_pairs(lj_ctx* ctx, long long cap, int* pi, int* pj, int* pimg, double* pr2) {
+    if (!ctx || cap < 0 || (cap > 0 && (!pi || !pj || !pimg || !pr2))) return -LJ_ERR_ARG;
+    if (ctx->p.force_kind == LJ_FORCE_NONE) return 0;
+    if (cudaSetDevice(ctx->p.device) != cudaSuccess) return -LJ_ERR_CUDA;
+    // make sure the list reflects the current positions
+    int one = 1;
+    if (cudaMemcpyAsync(&ctx->sc->need_rebuild, &one, sizeof(int), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+        return -LJ_ERR_CUDA;
+    int rc = launch_rebuild(ctx);
+    if (rc) return -rc;
+    int* di = nullptr; int* dj = nullptr; int* dm = nullptr; double* dr = nullptr;
+    unsigned long long* counter = nullptr;
+    long long c = cap > 0 ? cap : 1;
+    cudaError_t e = cudaMalloc(&di, sizeof(int) * c);
+    if (e == cudaSuccess) e = cudaMalloc(&dj, sizeof(int) * c);
+    if (e == cudaSuccess) e = cudaMalloc(&dm, sizeof(int) * c);
+    if (e == cudaSuccess) e = cudaMalloc(&dr, sizeof(double) * c);
+    if (e == cudaSuccess) e = cudaMalloc(&counter, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), ctx->stream);
+    unsigned long long total = 0;
+    if (e == cudaSuccess) {
+        if (ctx->small_box)
+            debug_pairs_kernel<true><<<ctx->nblocks, kThreads, 0, ctx->stream>>>(
+                ctx->N, ctx->pos, ctx->nbr, ctx->cnt, ctx->ids, ctx->pp, cap, di, dj, dm, dr, counter);
+        else
+            debug_pairs_kernel<false><<<ctx->nblocks, kThreads, 0, ctx->stream>>>(
+                ctx->N, ctx->pos, ctx->nbr, ctx->cnt, ctx->ids, ctx->pp, cap, di, dj, dm, dr, counter);
+        e = cudaGetLastError();
+        ++ctx->launches;
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&total, counter, sizeof total, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    long long n = std::min<long long>((long long)total, cap);
+    if (e == cudaSuccess && n > 0) {
+        e = cudaMemcpy(pi, di, sizeof(int) * n, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(pj, dj, sizeof(int) * n, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(pimg, dm, sizeof(int) * n, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(pr2, dr, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    }
+    cudaFree(di); cudaFree(dj); cudaFree(dm); cudaFree(dr); cudaFree(counter);
+    if (e != cudaSuccess) {
+        std::snprintf(ctx->err, sizeof ctx->err, "debug_pairs: %s", cudaGetErrorString(e));
+        return -LJ_ERR_CUDA;
+    }
+    int st = read_flags(ctx);
+    if (st) return -st;
+    return (long long)total;
+}
+
+int lj_gpu_get_stats(const lj_ctx* ctx_c, lj_stats* out) {
+    lj_ctx* ctx = const_cast<lj_ctx*>(ctx_c);
+    if (!ctx || !out) return LJ_ERR_ARG;
+    CK(cudaSetDevice(ctx->p.device));
+    Scalars h;
+    CK(cudaMemcpyAsync(&h, ctx->sc, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    out->steps = h.steps;
+    out->list_builds = h.builds;
+    out->neighbor_capacity = ctx->cap;
+    for (int k = 0; k < 3; ++k) out->list_cells[k] = ctx->list_grid.n[k];
+    out->max_neighbors = h.max_count;
+    out->small_box = ctx->small_box ? 1 : 0;
+    out->skin = ctx->skin;
+    out->kernel_launches = ctx->launches;
+    return LJ_OK;
+}
+
+int lj_gpu_rdf(lj_ctx* ctx, int nbins, double rmax, unsigned long long* hist) {
+    if (!ctx || nbins < 1 || !hist || !(rmax > 0)) return set_err(ctx, LJ_ERR_ARG, "bad rdf arguments");
+    for (int k = 0; k < 3; ++k)
+        if (rmax > 0.5 * ctx->pp.L[k]) return set_err(ctx, LJ_ERR_ARG, "rmax exceeds half the box");
+    return rdf_launch(ctx->N, ctx->pos, ctx->pp, nbins, rmax, hist, ctx->stream, ctx->err, sizeof ctx->err,
+                      &ctx->launches);
+}
+
+}  // extern "C"
+
+extern "C" {
+
+void* lj_gpu_stream(lj_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int lj_gpu_step_async(lj_ctx* ctx, int nsteps) {
+    if (!ctx || nsteps < 0) return set_err(ctx, LJ_ERR_ARG, "bad step arguments");
+    CK(cudaSetDevice(ctx->p.device));
+    for (int s = 0; s < nsteps; ++s) {
+        int rc = launch_step(ctx, s % ctx->ring_cap);
+        if (rc) return rc;
+    }
+    return LJ_OK;
+}
+
+int lj_gpu_synchronize(lj_ctx* ctx) {
+    if (!ctx) return LJ_ERR_ARG;
+    CK(cudaSetDevice(ctx->p.device));
+    return read_flags(ctx);
+}
+
+int lj_gpu_step_timed(lj_ctx* ctx, int nsteps, lj_phase_times* out) {
+    if (!ctx || nsteps < 0 || !out) return set_err(ctx, LJ_ERR_ARG, "bad step arguments");
+    CK(cudaSetDevice(ctx->p.device));
+    std::memset(out, 0, sizeof *out);
+    cudaEvent_t ev[5];
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    Scalars before;
+    CK(cudaMemcpy(&before, ctx->sc, sizeof before, cudaMemcpyDeviceToHost));
+    bool forces = ctx->p.force_kind != LJ_FORCE_NONE;
+    for (int s = 0; s < nsteps; ++s) {
+        int slot = s % ctx->ring_cap, rc;
+        CK(cudaEventRecord(ev[0], ctx->stream));
+        if ((rc = launch_kick_drift(ctx))) return rc;
+        CK(cudaEventRecord(ev[1], ctx->stream));
+        if (forces && (rc = launch_rebuild(ctx))) return rc;
+        CK(cudaEventRecord(ev[2], ctx->stream));
+        if (forces) {
+            if ((rc = launch_force(ctx, true))) return rc;
+        } else {
+            kick_measure_kernel<<<ctx->nblocks, kThreads, 0, ctx->stream>>>(ctx->N, soa_of(ctx->soa, ctx->N),
+                                                                             ctx->pp.dt, 1, ctx->partials);
+            CKL();
+        }
+        CK(cudaEventRecord(ev[3], ctx->stream));
+        finalize_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->partials, ctx->nblocks, ctx->N, ctx->pp.dt, 0,
+                                                     forces ? 1 : 0, ctx->sc, ctx->ring + 7 * (size_t)slot);
+        CKL();
+        CK(cudaEventRecord(ev[4], ctx->stream));
+        CK(cudaEventSynchronize(ev[4]));
+        float ms[4];
+        for (int q = 0; q < 4; ++q) CK(cudaEventElapsedTime(&ms[q], ev[q], ev[q + 1]));
+        out->kick_drift_ms += ms[0];
+        out->rebuild_ms += ms[1];
+        out->force_ms += ms[2];
+        out->finalize_ms += ms[3];
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    Scalars after;
+    CK(cudaMemcpy(&after, ctx->sc, sizeof after, cudaMemcpyDeviceToHost));
+    out->steps = nsteps;
+    out->rebuilds = after.builds - before.builds;
+    return read_flags(ctx);
+}
+
+}  // extern "C"

@@ -1,0 +1,584 @@
+// lj_kernels.cuh -- kernels of the single-system engine (FP64 drop-in path and
+// the shared binning / neighbour-list machinery).
+//
+// Device layout (HBM), all in cell-sorted slot order and re-sorted at every
+// neighbour-list build:
+//   pos   double4[N]       x, y, z, 0 -- gathered by neighbours, one 32-byte sector each
+//   soa   double[9][N]     vx vy vz | dx dy dz (displacement) | fx fy fz, coalesced per atom
+//   ids   int[N]           slot -> atom id (the reference's column index)
+//   bd    double[3][N]     displacement at the last list build (skin criterion)
+//   nbr   uint32[cap][N]   neighbour list, transposed so entry k of all atoms is contiguous;
+//                          slot in the low 27 bits, a 5-bit code above it
+//   cnt   int[N]           neighbour count
+#pragma once
+
+#include "lj_common.cuh"
+
+namespace ljb {
+
+enum SoaField { VX = 0, VY, VZ, DX, DY, DZ, FX, FY, FZ, SOA_FIELDS };
+
+struct Soa {
+    double* p;
+    int N;
+    __device__ __forceinline__ double& at(int f, int i) const { return p[(size_t)f * N + i]; }
+};
+
+// Rebuild gate: evaluated identically by every kernel of the rebuild chain.
+struct Gate {
+    const Scalars* sc;
+    double thresh2;  // rebuild when max |d - d_build|^2 exceeds this
+    int always;      // small-box / zero-skin mode: rebuild every step
+    __device__ __forceinline__ bool open() const {
+        if (always || sc->need_rebuild) return true;
+        return __longlong_as_double((long long)sc->max_disp2) > thresh2;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Integration: integrator.cpp:62-88, first half (kick, drift, displacement, wrap)
+// ---------------------------------------------------------------------------
+template <bool PERIODIC, bool TRACK>
+static __global__ void __launch_bounds__(kThreads)
+kick_drift_kernel(int N, double4* __restrict__ pos, Soa s, const double* __restrict__ bd,
+                  PairParams pp, Scalars* sc) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double m = 0.0;
+    if (i < N) {
+        double4 x = pos[i];
+        double xs[3] = {x.x, x.y, x.z};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            double v = kick(s.at(VX + k, i), s.at(FX + k, i), pp.dt);
+            double inc = __dmul_rn(v, pp.dt);
+            double xn = __dadd_rn(xs[k], inc);
+            double dn = __dadd_rn(s.at(DX + k, i), inc);
+            if (PERIODIC) xn = wrap(xn, pp.L[k]);
+            s.at(VX + k, i) = v;
+            s.at(DX + k, i) = dn;
+            xs[k] = xn;
+            if (TRACK) {
+                double e = dn - bd[(size_t)k * N + i];
+                m = fma(e, e, m);
+            }
+        }
+        pos[i] = make_double4(xs[0], xs[1], xs[2], 0.0);
+    }
+    if (TRACK) {
+        m = warp_max(m);
+        if ((threadIdx.x & 31) == 0 && m > 0.0)
+            atomicMax(&sc->max_disp2, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+// Second half kick without a force calculation (LJ_FORCE_NONE), with the
+// measurement partial sums.
+static __global__ void __launch_bounds__(kThreads)
+kick_measure_kernel(int N, Soa s, double dt, int do_kick, double* __restrict__ partials) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[4] = {0, 0, 0, 0};
+    if (i < N) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            double v = s.at(VX + k, i);
+            if (do_kick) {
+                v = kick(v, s.at(FX + k, i), dt);
+                s.at(VX + k, i) = v;
+            }
+            acc[0] = fma(v, v, acc[0]);
+            double d = s.at(DX + k, i);
+            acc[3] = fma(d, d, acc[3]);
+        }
+    }
+    block_sum<4, kThreads>(acc);
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 4; ++q) partials[(size_t)blockIdx.x * 4 + q] = acc[q];
+}
+
+// ---------------------------------------------------------------------------
+// Cell binning (counting sort): particle_pair_filter.cpp:141-154
+// ---------------------------------------------------------------------------
+template <bool GATED>
+static __global__ void __launch_bounds__(kThreads)
+bin_count_kernel(int N, const double4* __restrict__ pos, Grid g, int* __restrict__ cell_of,
+                 int* __restrict__ rank, int* __restrict__ count, Gate gate) {
+    if (GATED && !gate.open()) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double4 x = pos[i];
+    int c = g.flat(cell_coord(x.x, g.ratio[0], g.n[0]), cell_coord(x.y, g.ratio[1], g.n[1]),
+                   cell_coord(x.z, g.ratio[2], g.n[2]));
+    cell_of[i] = c;
+    rank[i] = atomicAdd(&count[c], 1);
+}
+
+// Exclusive scan of count[0..n) into start[0..n]: tile sums, scan of tile sums, apply.
+template <bool GATED>
+static __global__ void __launch_bounds__(1024)
+scan_reduce_kernel(const int* __restrict__ count, int n, int* __restrict__ tile_sums, Gate gate) {
+    if (GATED && !gate.open()) return;
+    int base = blockIdx.x * kScanTile + threadIdx.x * 4;
+    int s = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) s += base + q < n ? count[base + q] : 0;
+    __shared__ int tot;
+    block_exclusive_scan<1024>(s, &tot);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = tot;
+}
+
+template <bool GATED>
+static __global__ void __launch_bounds__(1024)
+scan_tiles_kernel(int* __restrict__ tile_sums, int ntiles, Gate gate) {
+    if (GATED && !gate.open()) return;
+    int x = threadIdx.x < ntiles ? tile_sums[threadIdx.x] : 0;
+    __shared__ int tot;
+    int ex = block_exclusive_scan<1024>(x, &tot);
+    if (threadIdx.x < ntiles) tile_sums[threadIdx.x] = ex;
+}
+
+template <bool GATED>
+static __global__ void __launch_bounds__(1024)
+scan_apply_kernel(int* __restrict__ count, int n, const int* __restrict__ tile_sums,
+                  int* __restrict__ start, Gate gate) {
+    if (GATED && !gate.open()) return;
+    int base = blockIdx.x * kScanTile + threadIdx.x * 4;
+    int c[4];
+    int s = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        c[q] = base + q < n ? count[base + q] : 0;
+        s += c[q];
+    }
+    __shared__ int tot;
+    int ex = block_exclusive_scan<1024>(s, &tot) + tile_sums[blockIdx.x];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        if (base + q < n) {
+            start[base + q] = ex;
+            count[base + q] = 0;  // ready for the next binning
+        }
+        ex += c[q];
+    }
+    if (base < n && base + 4 >= n) start[n] = ex;
+}
+
+template <bool GATED>
+static __global__ void __launch_bounds__(kThreads)
+scatter_kernel(int N, const int* __restrict__ cell_of, const int* __restrict__ rank,
+               const int* __restrict__ start, int* __restrict__ order, Gate gate) {
+    if (GATED && !gate.open()) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    order[start[cell_of[i]] + rank[i]] = i;
+}
+
+// Order each cell's members by their previous slot.  Slots come from the last
+// sort, so the order is a fixed function of the trajectory and every run is
+// bit-reproducible without reading atom ids.  (The reference's own cell
+// contents, ascending atom id, are produced by lj_gpu_debug_cells.)
+template <bool GATED>
+static __global__ void __launch_bounds__(kThreads)
+cell_sort_kernel(int ncell, const int* __restrict__ start, int* __restrict__ order, Gate gate) {
+    if (GATED && !gate.open()) return;
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    int b = start[c], e = start[c + 1];
+    for (int k = b + 1; k < e; ++k) {
+        int v = order[k];
+        int q = k - 1;
+        while (q >= b && order[q] > v) {
+            order[q + 1] = order[q];
+            --q;
+        }
+        order[q + 1] = v;
+    }
+}
+
+// Gather the state into sorted order (into the scratch copies).
+static __global__ void __launch_bounds__(kThreads)
+gather_kernel(int N, const int* __restrict__ order, const double4* __restrict__ pos,
+              double4* __restrict__ pos_out, Soa s, Soa s_out, const int* __restrict__ ids,
+              int* __restrict__ ids_out, double* __restrict__ bd, Gate gate) {
+    if (!gate.open()) return;
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= N) return;
+    int o = order[k];
+    pos_out[k] = pos[o];
+#pragma unroll
+    for (int f = 0; f < SOA_FIELDS; ++f) s_out.at(f, k) = s.at(f, o);
+    ids_out[k] = ids[o];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) bd[(size_t)q * N + k] = s.at(DX + q, o);
+}
+
+// Copy the sorted state back and write the FP32 position copy used by the list build.
+static __global__ void __launch_bounds__(kThreads)
+copy_back_kernel(int N, const double4* __restrict__ pos_in, double4* __restrict__ pos, Soa s_in,
+                 Soa s, const int* __restrict__ ids_in, int* __restrict__ ids, float4* __restrict__ posf,
+                 Gate gate) {
+    if (!gate.open()) return;
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= N) return;
+    double4 x = pos_in[k];
+    pos[k] = x;
+    posf[k] = make_float4((float)x.x, (float)x.y, (float)x.z, 0.f);
+#pragma unroll
+    for (int f = 0; f < SOA_FIELDS; ++f) s.at(f, k) = s_in.at(f, k);
+    ids[k] = ids_in[k];
+}
+
+// Neighbour list over the 27-cell stencil of the list grid.
+//
+// Layout: groups of 4 entries, group g of atom i at nbr4[g * N + i] (one 16-byte
+// load per group, coalesced across a warp); the tail of the last group is
+// padded with the ghost slot N, which sits far outside every box.  An entry
+// holds the slot in its low 27 bits and a 5-bit code above: the lattice image
+// in SMALL mode (grids under 3 cells per axis, rebuilt every step), otherwise
+// the stencil offset (the pair kernels recompute the minimum image each step).
+//
+// The candidate test runs in FP32 on box coordinates against a radius widened
+// by 8 * L * 2^-24, so the list is a superset of the FP64 pair set; the pair
+// kernels apply the exact test.
+template <bool SMALL>
+static __global__ void __launch_bounds__(kThreads)
+build_list_kernel(int N, const double4* __restrict__ pos, const float4* __restrict__ posf, Grid g,
+                  const int* __restrict__ start,
+                  float3 Lf, float cut2, int cap, uint4* __restrict__ nbr4,
+                  int* __restrict__ cnt, Scalars* sc, Gate gate) {
+    if (!gate.open()) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int n = 0;
+    unsigned* nbr = reinterpret_cast<unsigned*>(nbr4);
+    if (i < N) {
+        float4 xi = posf[i];
+        // the home cell comes from the FP64 position, exactly as the binning placed the atom
+        double4 xd = pos[i];
+        int ci[3] = {cell_coord(xd.x, g.ratio[0], g.n[0]), cell_coord(xd.y, g.ratio[1], g.n[1]),
+                     cell_coord(xd.z, g.ratio[2], g.n[2])};
+        for (int a = -1; a <= 1; ++a) {
+            int na = ci[0] + a, ia = na < 0 ? -1 : (na >= g.n[0] ? 1 : 0);
+            na -= ia * g.n[0];
+            for (int b = -1; b <= 1; ++b) {
+                int nb = ci[1] + b, ib = nb < 0 ? -1 : (nb >= g.n[1] ? 1 : 0);
+                nb -= ib * g.n[1];
+                for (int c = -1; c <= 1; ++c) {
+                    int nc = ci[2] + c, ic = nc < 0 ? -1 : (nc >= g.n[2] ? 1 : 0);
+                    nc -= ic * g.n[2];
+                    int cell = g.flat(na, nb, nc);
+                    float sx = ia * Lf.x, sy = ib * Lf.y, sz = ic * Lf.z;
+                    unsigned code = SMALL ? (unsigned)image_code(ia, ib, ic)
+                                          : (unsigned)image_code(a, b, c);
+                    int e = start[cell + 1];
+                    for (int j = start[cell]; j < e; ++j) {
+                        float4 xj = posf[j];
+                        float dx = (xi.x - xj.x) - sx;
+                        float dy = (xi.y - xj.y) - sy;
+                        float dz = (xi.z - xj.z) - sz;
+                        if (fmaf(dz, dz, fmaf(dy, dy, dx * dx)) < cut2 && j != i) {
+                            if (n < cap) nbr[((size_t)(n >> 2) * N + i) * 4 + (n & 3)] = (unsigned)j | (code << kSlotBits);
+                            ++n;
+                        }
+                    }
+                }
+            }
+        }
+        int m = n < cap ? n : cap;
+        cnt[i] = m;
+        for (int k = m; k < ((m + 3) & ~3); ++k)  // ghost padding (code 13: no image, no offset)
+            nbr[((size_t)(k >> 2) * N + i) * 4 + (k & 3)] = (unsigned)N | (13u << kSlotBits);
+    }
+    // block max of n -> sc->max_count; overflow flag
+    int m = n;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) m = max(m, __shfl_down_sync(0xffffffffu, m, off));
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&sc->max_count, m);
+        if (m > cap) atomicExch(&sc->overflow, 1);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd((unsigned long long*)&sc->builds, 1ull);
+}
+
+// ---------------------------------------------------------------------------
+// FP64 pair force: full shell over the neighbour list (each atom sums its own
+// row, so per-atom sums are deterministic and need no atomics), LJ spline of
+// lennard_jones_force.cpp:107-119.  KICK fuses the second half kick
+// (integrator.cpp:82) and the measurement partial sums into the epilogue.
+//
+// The loop runs over groups of 4 neighbours: the next group's indices are
+// loaded (streaming, evict-first) while the current group's 4 positions are
+// gathered and its 4 pairs evaluated without branches, the cutoff applied as a
+// select.  That keeps several independent memory requests in flight per warp.
+// ---------------------------------------------------------------------------
+enum { KIND_LJ = 1, KIND_CONST = 2 };
+
+// 1/x: the hardware's approximate FP64 reciprocal refined by two Newton-Raphson
+// steps y <- y + y (1 - x y) (quadratic convergence from the ~2^-20 seed to
+// the last bit of the result).
+__device__ __forceinline__ double rcp_nr(double x) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
+}
+
+template <bool SMALL>
+__device__ __forceinline__ void separation(const double4& xi, const double4& xj, unsigned e, bool near,
+                                           const PairParams& pp, double& dx, double& dy, double& dz) {
+    dx = __dsub_rn(xi.x, xj.x);
+    dy = __dsub_rn(xi.y, xj.y);
+    dz = __dsub_rn(xi.z, xj.z);
+    if (SMALL) {
+        int code = (int)(e >> kSlotBits);
+        int ia = code / 9 - 1, ib = (code / 3) % 3 - 1, ic = code % 3 - 1;
+        dx = __dsub_rn(dx, ia * pp.L[0]);
+        dy = __dsub_rn(dy, ib * pp.L[1]);
+        dz = __dsub_rn(dz, ic * pp.L[2]);
+    } else if (near) {
+        // minimum image; identical to the reference's stencil image for every
+        // pair inside the cutoff (the list grid has >= 3 cells per axis)
+        if ((__double2hiint(dx) & 0x7fffffff) > pp.halfL_hi[0]) dx = __dsub_rn(dx, copysign(pp.L[0], dx));
+        if ((__double2hiint(dy) & 0x7fffffff) > pp.halfL_hi[1]) dy = __dsub_rn(dy, copysign(pp.L[1], dy));
+        if ((__double2hiint(dz) & 0x7fffffff) > pp.halfL_hi[2]) dz = __dsub_rn(dz, copysign(pp.L[2], dz));
+    }
+}
+
+template <int KIND>
+__device__ __forceinline__ void pair_fp64(const PairParams& pp, double r2, double& f, double& V, double& W) {
+    if (KIND == KIND_LJ) {
+        bool hit = r2 < pp.rc2;
+        double ir2 = rcp_nr(r2);
+        double ir6 = ir2 * ir2 * ir2;
+        double x = r2 * pp.inv_rc2;
+        double v = fma(4.0 * ir6, ir6 - 1.0, fma(pp.beta, x - 1.0, pp.alpha));
+        double w = fma(24.0 * ir6, fma(2.0, ir6, -1.0), -2.0 * pp.beta * x);
+        f = hit ? w * ir2 : 0.0;
+        V = hit ? v : 0.0;
+        W = hit ? w : 0.0;
+    } else {
+        // tests/cpp/mock/constant_short_range_force.cpp:35-53
+        double norm = sqrt(r2);
+        bool hit = r2 < pp.rc2 && norm < pp.rc;
+        V = hit ? pp.strength * (pp.rc - norm) : 0.0;
+        W = hit ? pp.strength * norm : 0.0;
+        f = hit ? W / (norm * norm) : 0.0;
+    }
+}
+
+template <int KIND, bool SMALL, bool KICK>
+static __global__ void __launch_bounds__(kThreads, 4)
+force_fp64_kernel(int N, const double4* __restrict__ pos, Soa s, const uint4* __restrict__ nbr4,
+                  const int* __restrict__ cnt, PairParams pp, double* __restrict__ partials) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[4] = {0, 0, 0, 0};  // sum v^2, sum pe_i, sum w_i, sum d^2
+    if (i < N) {
+        const double4 xi = pos[i];
+        bool near = !(xi.x >= pp.near_lo && xi.x < pp.near_hi[0] && xi.y >= pp.near_lo &&
+                      xi.y < pp.near_hi[1] && xi.z >= pp.near_lo && xi.z < pp.near_hi[2]);
+        double fx = 0, fy = 0, fz = 0, pe = 0, w = 0;
+        int ng = (cnt[i] + 3) >> 2;
+        uint4 cur = ng > 0 ? __ldcs(&nbr4[i]) : make_uint4(0, 0, 0, 0);
+        for (int g = 0; g < ng; ++g) {
+            uint4 nxt = g + 1 < ng ? __ldcs(&nbr4[(size_t)(g + 1) * N + i]) : cur;
+            unsigned e[4] = {cur.x, cur.y, cur.z, cur.w};
+            double4 q[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) q[u] = pos[e[u] & kSlotMask];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                double dx, dy, dz, f, V, W;
+                separation<SMALL>(xi, q[u], e[u], near, pp, dx, dy, dz);
+                pair_fp64<KIND>(pp, norm2(dx, dy, dz), f, V, W);
+                fx = fma(f, dx, fx);
+                fy = fma(f, dy, fy);
+                fz = fma(f, dz, fz);
+                pe += V;
+                w += W;
+            }
+            cur = nxt;
+        }
+        s.at(FX, i) = fx;
+        s.at(FY, i) = fy;
+        s.at(FZ, i) = fz;
+        acc[1] = pe;
+        acc[2] = w;
+        if (KICK) {
+            double f3[3] = {fx, fy, fz};
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                double v = kick(s.at(VX + k, i), f3[k], pp.dt);
+                s.at(VX + k, i) = v;
+                acc[0] = fma(v, v, acc[0]);
+                double d = s.at(DX + k, i);
+                acc[3] = fma(d, d, acc[3]);
+            }
+        }
+    }
+    block_sum<4, kThreads>(acc);
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 4; ++q) partials[(size_t)blockIdx.x * 4 + q] = acc[q];
+}
+
+// ---------------------------------------------------------------------------
+// Step finalisation: sum the per-block partials in a fixed order and publish
+// ThermodynamicMeasurement::Result (measurements.hpp:59-70).
+// mode 0: after a step (t += dt); 1: after a force evaluation (PE, W only);
+// 2: measurement of the current state.
+// ---------------------------------------------------------------------------
+static __global__ void __launch_bounds__(1024)
+finalize_kernel(const double* __restrict__ partials, int nblocks, int N, double dt, int mode,
+                int forces_valid, Scalars* sc, double* __restrict__ out /* 7 doubles */) {
+    double acc[4] = {0, 0, 0, 0};
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[q] += partials[(size_t)b * 4 + q];
+    block_sum<4, 1024>(acc);
+    if (threadIdx.x == 0) {
+        if (forces_valid) {
+            sc->pe = 0.5 * acc[1];
+            sc->vir = 0.5 * acc[2];
+        }
+        if (mode == 0) {
+            sc->t = sc->t + dt;  // integrator.cpp:85
+            sc->steps += 1;
+        }
+        if (mode != 1) {
+            double ke = 0.5 * acc[0];
+            double rec[7];
+            rec[0] = sc->t;
+            rec[1] = ke;
+            rec[2] = sc->pe;
+            rec[3] = sc->pe + ke;
+            rec[4] = sc->vir;
+            rec[5] = (2. / 3.) * ke / (double)N;
+            rec[6] = acc[3] / (double)N;
+            for (int q = 0; q < 7; ++q) out[q] = rec[q];
+            if (!isfinite(ke) || !isfinite(sc->pe) || !isfinite(sc->vir)) sc->nonfinite = 1;
+        } else if (!isfinite(sc->pe) || !isfinite(sc->vir)) {
+            sc->nonfinite = 1;
+        }
+        sc->max_disp2 = 0ull;
+        sc->need_rebuild = 0;
+    }
+}
+
+static __global__ void __launch_bounds__(kThreads)
+scale_kernel(int N, Soa s, double factor) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) s.at(VX + k, i) = __dmul_rn(s.at(VX + k, i), factor);
+}
+
+// set_temperature (transformations.cpp:94-116): the factor is computed on the
+// device from the KE of the record written by the preceding measurement.
+static __global__ void set_temperature_factor_kernel(const double* rec, double target, double* factor) {
+    *factor = sqrt(target / rec[5]);
+}
+
+static __global__ void __launch_bounds__(kThreads)
+scale_from_device_kernel(int N, Soa s, const double* __restrict__ factor) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double f = *factor;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) s.at(VX + k, i) = __dmul_rn(s.at(VX + k, i), f);
+}
+
+// ---------------------------------------------------------------------------
+// Host <-> device layout conversion (atom-id order <-> sorted slots)
+// ---------------------------------------------------------------------------
+static __global__ void unpack_kernel(int N, const double* __restrict__ in, int stride, int field,
+                              double4* __restrict__ pos, Soa s, int* __restrict__ ids) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double* p = in + (size_t)i * stride;
+    if (field < 0) {
+        pos[i] = make_double4(p[0], p[1], p[2], 0.0);
+        ids[i] = i;
+    } else {
+        for (int k = 0; k < 3; ++k) s.at(field + k, i) = p[k];
+    }
+}
+
+static __global__ void pack_kernel(int N, double* __restrict__ out, int stride, int field,
+                            const double4* __restrict__ pos, Soa s, const int* __restrict__ ids) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= N) return;
+    double* p = out + (size_t)ids[k] * stride;
+    double v[3];
+    if (field < 0) {
+        double4 x = pos[k];
+        v[0] = x.x; v[1] = x.y; v[2] = x.z;
+    } else {
+        for (int q = 0; q < 3; ++q) v[q] = s.at(field + q, k);
+    }
+    for (int q = 0; q < 3; ++q) p[q] = v[q];
+    if (stride == 4) p[3] = 0.0;
+}
+
+// Reference binning for the debug API: cell of each atom id, and members as ids.
+static __global__ void debug_members_kernel(int N, const int* __restrict__ cell_of_slot,
+                                     const int* __restrict__ rank, const int* __restrict__ start,
+                                     const int* __restrict__ ids, int* __restrict__ members,
+                                     int* __restrict__ cell_of_id) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= N) return;
+    members[start[cell_of_slot[k]] + rank[k]] = ids[k];
+    cell_of_id[ids[k]] = cell_of_slot[k];
+}
+
+static __global__ void sort_members_kernel(int ncell, const int* __restrict__ start, int* __restrict__ m) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    for (int k = start[c] + 1; k < start[c + 1]; ++k) {
+        int v = m[k], q = k - 1;
+        while (q >= start[c] && m[q] > v) {
+            m[q + 1] = m[q];
+            --q;
+        }
+        m[q + 1] = v;
+    }
+}
+
+// The in-cutoff pair set as seen by the force kernel (i < j by id).
+template <bool SMALL>
+static __global__ void debug_pairs_kernel(int N, const double4* __restrict__ pos,
+                                   const uint4* __restrict__ nbr4, const int* __restrict__ cnt,
+                                   const int* __restrict__ ids, PairParams pp, long long cap,
+                                   int* oi, int* oj, int* oimg, double* or2,
+                                   unsigned long long* counter) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double4 xi = pos[i];
+    const unsigned* nbr = reinterpret_cast<const unsigned*>(nbr4);
+    for (int k = 0; k < cnt[i]; ++k) {
+        unsigned e = nbr[((size_t)(k >> 2) * N + i) * 4 + (k & 3)];
+        int j = (int)(e & kSlotMask);
+        if (ids[i] >= ids[j]) continue;
+        double4 xj = pos[j];
+        double d[3] = {__dsub_rn(xi.x, xj.x), __dsub_rn(xi.y, xj.y), __dsub_rn(xi.z, xj.z)};
+        int img[3] = {0, 0, 0};
+        if (SMALL) {
+            int code = (int)(e >> kSlotBits);
+            img[0] = code / 9 - 1; img[1] = (code / 3) % 3 - 1; img[2] = code % 3 - 1;
+        } else {
+            for (int q = 0; q < 3; ++q)
+                if ((__double2hiint(d[q]) & 0x7fffffff) > pp.halfL_hi[q]) img[q] = d[q] > 0 ? 1 : -1;
+        }
+        for (int q = 0; q < 3; ++q) d[q] = __dsub_rn(d[q], img[q] * pp.L[q]);
+        double r2 = norm2(d[0], d[1], d[2]);
+        if (r2 < pp.rc2) {
+            unsigned long long slot = atomicAdd(counter, 1ull);
+            if ((long long)slot < cap) {
+                oi[slot] = ids[i];
+                oj[slot] = ids[j];
+                oimg[slot] = image_code(img[0], img[1], img[2]);
+                or2[slot] = r2;
+            }
+        }
+    }
+}
+
+}  // namespace ljb

@@ -1,0 +1,77 @@
+"""The C-ABI library loads and exports every symbol include/lj_gpu.h declares (no GPU calls)."""
+
+import ctypes
+import pathlib
+import re
+
+import numpy as np
+import pytest
+
+ROOT = pathlib.Path(__file__).resolve().parents[1]
+
+
+def declared_symbols():
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        names |= set(re.findall(r"\b(lj_\w+)\s*\(", text))
+    return sorted(names)
+
+
+def test_header_declares_entry_points():
+    names = declared_symbols()
+    for must in ("lj_gpu_create", "lj_gpu_step", "lj_gpu_compute_forces", "lj_gpu_debug_pairs",
+                 "lj_gpu_debug_cells", "lj_gpu_rdf", "lj_initial_condition"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    from lennardjonesium import _native
+    L = _native.lib()
+    for name in declared_symbols():
+        assert hasattr(L, name), name
+        assert name in _native.SIGNATURES, name
+
+
+def test_status_strings_and_default_params():
+    from lennardjonesium import _native
+    L = _native.lib()
+    assert L.lj_gpu_status_string(0) == b"ok"
+    assert L.lj_gpu_status_string(5) == b"neighbour list capacity exceeded"
+    p = _native.Params()
+    L.lj_gpu_default_params(ctypes.byref(p))
+    assert p.cutoff_distance == 2.5 and p.time_delta == 0.005 and p.periodic == 1
+
+
+def test_create_rejects_bad_arguments():
+    """Argument checks run on the host before any device call."""
+    from lennardjonesium import _native
+    L = _native.lib()
+    p = _native.Params()
+    L.lj_gpu_default_params(ctypes.byref(p))
+    ctx = ctypes.c_void_p()
+    p.particle_count = 0
+    assert L.lj_gpu_create(ctypes.byref(p), ctypes.byref(ctx)) == _native.LJ_ERR_ARG
+    p.particle_count = 10
+    for k in range(3):
+        p.box[k] = 2.0  # box below the cutoff (particle_pair_filter.cpp:61-64)
+    assert L.lj_gpu_create(ctypes.byref(p), ctypes.byref(ctx)) == _native.LJ_ERR_ARG
+    for k in range(3):
+        p.box[k] = 10.0
+    p.cutoff_distance = 1.0  # rc^2 <= 2^(1/3) (lennard_jones_force.cpp:45)
+    assert L.lj_gpu_create(ctypes.byref(p), ctypes.byref(ctx)) == _native.LJ_ERR_ARG
+    p.cutoff_distance = 2.5
+    p.periodic = 0  # forces without the periodic boundary are not a reference configuration
+    assert L.lj_gpu_create(ctypes.byref(p), ctypes.byref(ctx)) == _native.LJ_ERR_ARG
+
+
+def test_host_initial_condition_matches_oracle():
+    """The library's InitialCondition equals the oracle's (same seed contract)."""
+    import ljref
+    from lennardjonesium import initial_condition
+    for N, T, rho, seed in [(500, 0.5, 0.8, 117208264), (864, 0.722, 0.8442, 5489), (100, 0.6, 1.0, 17)]:
+        x, v, L = initial_condition(N, T, rho, seed)
+        xo, vo, Lo = ljref.initial_state(N, T, rho, seed)
+        assert L == Lo
+        assert np.array_equal(x, xo)
+        assert np.allclose(v, vo, rtol=0, atol=1e-14)
