@@ -189,6 +189,30 @@ int lj_gpu_step_timed(lj_ctx* ctx, int nsteps, lj_phase_times* out);
  * (TFLOP/s, 2 flops per FMA): the roofline denominators of the pair kernels. */
 int lj_gpu_fma_peaks(int device, double* fp64_tflops, double* fp32_tflops);
 
+/* Allocation-free radial distribution histogram.  No counterpart in the
+ * reference (it has no RDF, and it never runs on a GPU).
+ *
+ * For callers that may not call cudaMalloc -- an application whose GPU memory
+ * belongs to its own pool allocator, or a per-step analysis hook in a loop
+ * that cannot afford cudaMalloc's latency and implicit synchronisation.  The
+ * caller passes device buffers it already owns:
+ *   pos   device, N x 4 doubles (SystemState layout), 16-byte aligned
+ *   hist  device, nbins unsigned 64-bit counts (overwritten)
+ *   box   host, 3 edge lengths; rmax <= min(box) / 2
+ *   stream  cudaStream_t to run on (NULL: the legacy default stream)
+ * The work is enqueued on the stream and the call returns without waiting.
+ * Counts are those of lj_gpu_rdf.  Limits: N <= 131072, nbins <= 12288, and at
+ * most 32768 cells of edge >= rmax; larger inputs return LJ_ERR_ARG.
+ *
+ * Scratch is one fixed device array inside this library (about 5.3 MB, held on
+ * every GPU that loads the library until the process exits).  The first call
+ * on a device looks up that array's device address (cudaGetSymbolAddress), so
+ * make the first call on each device before any stream capture.  Calls share
+ * the array: calls whose GPU work overlaps (other streams, other threads) race
+ * and must be serialised by the caller. */
+int lj_gpu_rdf_noalloc(const double* pos, int N, const double* box, int nbins, double rmax,
+                       unsigned long long* hist, void* stream);
+
 /* engine::InitialCondition (engine/initial_condition.cpp:49-104,
  * tools/cubic_lattice.cpp:38-86): FCC positions and libstdc++-seeded
  * Maxwell-Boltzmann velocities with zero momentum and angular momentum,

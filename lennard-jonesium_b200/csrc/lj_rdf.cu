@@ -10,6 +10,8 @@
 // order); smaller boxes use all pairs.  Each block accumulates a shared-memory
 // histogram and adds it to the global 64-bit histogram once.
 
+#include <atomic>
+#include <cstdint>
 #include <cstdio>
 
 #include "lj_mixed.cuh"
@@ -178,3 +180,118 @@ int rdf_launch(int N, const double4* pos, const PairParams& pp, int nbins, doubl
 }
 
 }  // namespace ljb
+
+namespace ljb {
+
+// ---------------------------------------------------------------------------
+// Allocation-free RDF entry point.
+//
+// For callers that may not call cudaMalloc: an application whose GPU memory is
+// owned by its own pool allocator (a deep-learning framework, for instance,
+// whose caching allocator must see every allocation), or a per-step analysis
+// hook in a time-critical loop, where cudaMalloc's latency and the implicit
+// device-wide synchronisation that cudaMalloc/cudaFree can cause are not
+// acceptable.  They pass device buffers they already own for the positions and
+// the histogram; the cell-list scratch comes from the fixed device array below.
+//
+// The array is a file-scope __device__ variable: every GPU that loads this
+// library holds it (about 5.3 MB) until the process exits.  All calls on a
+// device share it and it keeps the last call's contents; each call clears what
+// must start at zero (the cell counts and the output histogram) on its stream.
+// Calls whose work overlaps on the GPU (different streams, or several host
+// threads) race on the shared array: serialise them.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+constexpr int kNoAllocMaxAtoms = 131072;
+constexpr int kNoAllocMaxCells = 32768;
+constexpr int kNoAllocMaxBins = 12288;  // 48 KB shared-memory histogram, no attribute change needed
+constexpr size_t kOffSorted = 0;
+constexpr size_t kOffCellOf = kOffSorted + sizeof(double4) * kNoAllocMaxAtoms;
+constexpr size_t kOffRank = kOffCellOf + sizeof(int) * kNoAllocMaxAtoms;
+constexpr size_t kOffCount = kOffRank + sizeof(int) * kNoAllocMaxAtoms;
+constexpr size_t kOffStart = kOffCount + sizeof(int) * kNoAllocMaxCells;
+constexpr size_t kOffTiles = kOffStart + sizeof(int) * (kNoAllocMaxCells + 256);
+constexpr size_t kNoAllocBytes = kOffTiles + sizeof(int) * kMaxScanTiles;
+static_assert(kOffCellOf % 256 == 0 && kOffRank % 256 == 0 && kOffCount % 256 == 0 &&
+              kOffStart % 256 == 0 && kOffTiles % 256 == 0, "scratch sub-buffers must stay aligned");
+
+__device__ __align__(256) unsigned char g_rdf_scratch[kNoAllocBytes];
+
+constexpr int kMaxDevices = 64;
+std::atomic<unsigned char*> g_scratch_addr[kMaxDevices];
+
+// Device address of g_rdf_scratch on the current device (looked up once per device).
+int scratch_address(unsigned char** out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 2;
+    unsigned char* p = g_scratch_addr[dev].load();
+    if (!p) {
+        void* q = nullptr;
+        if (cudaGetSymbolAddress(&q, g_rdf_scratch) != cudaSuccess || !q) return 2;
+        p = static_cast<unsigned char*>(q);
+        g_scratch_addr[dev].store(p);
+    }
+    *out = p;
+    return 0;
+}
+
+}  // namespace
+
+}  // namespace ljb
+
+extern "C" int lj_gpu_rdf_noalloc(const double* pos, int N, const double* box, int nbins, double rmax,
+                                  unsigned long long* hist, void* stream_handle) {
+    using namespace ljb;
+    if (!pos || !box || !hist || N < 1 || nbins < 1 || !(rmax > 0)) return 1;  // LJ_ERR_ARG
+    if (N > kNoAllocMaxAtoms || nbins > kNoAllocMaxBins) return 1;
+    if ((reinterpret_cast<uintptr_t>(pos) & 15) != 0) return 1;
+    PairParams pp{};
+    for (int k = 0; k < 3; ++k) {
+        if (!(box[k] > 0) || rmax > 0.5 * box[k]) return 1;
+        pp.L[k] = box[k];
+        pp.halfL[k] = 0.5 * box[k];
+    }
+    Grid g;
+    int nmin = 1 << 30;
+    for (int k = 0; k < 3; ++k) {
+        g.n[k] = (int)floor(pp.L[k] / rmax);
+        if (g.n[k] < 1) g.n[k] = 1;
+        g.ratio[k] = (double)g.n[k] / pp.L[k];
+        nmin = g.n[k] < nmin ? g.n[k] : nmin;
+    }
+    long long nc = (long long)g.n[0] * g.n[1] * g.n[2];
+    bool cells = nmin >= 3;
+    if (cells && nc > kNoAllocMaxCells) return 1;
+    unsigned char* base = nullptr;
+    if (scratch_address(&base)) return 2;  // LJ_ERR_CUDA
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_handle);
+    const double4* p4 = reinterpret_cast<const double4*>(pos);
+    double rmax2 = rmax * rmax, inv_dr = (double)nbins / rmax;
+    size_t shm = sizeof(unsigned) * nbins;
+    int blocks = (N + kThreads - 1) / kThreads;
+    if (cudaMemsetAsync(hist, 0, sizeof(unsigned long long) * nbins, stream) != cudaSuccess) return 2;
+    if (!cells) {
+        rdf_all_pairs_kernel<<<blocks, kThreads, shm, stream>>>(N, p4, pp, rmax2, inv_dr, nbins, hist);
+    } else {
+        double4* sorted = reinterpret_cast<double4*>(base + kOffSorted);
+        int* cell_of = reinterpret_cast<int*>(base + kOffCellOf);
+        int* rank = reinterpret_cast<int*>(base + kOffRank);
+        int* count = reinterpret_cast<int*>(base + kOffCount);
+        int* start = reinterpret_cast<int*>(base + kOffStart);
+        int* tiles = reinterpret_cast<int*>(base + kOffTiles);
+        int ncell = (int)nc;
+        int ntiles = (ncell + kScanTile - 1) / kScanTile;
+        if (cudaMemsetAsync(count, 0, sizeof(int) * ncell, stream) != cudaSuccess) return 2;
+        Gate open{};
+        open.always = 1;
+        rdf_bin_kernel<<<blocks, kThreads, 0, stream>>>(N, p4, g, cell_of, rank, count);
+        scan_reduce_kernel<false><<<ntiles, 1024, 0, stream>>>(count, ncell, tiles, open);
+        scan_tiles_kernel<false><<<1, 1024, 0, stream>>>(tiles, ntiles, open);
+        scan_apply_kernel<false><<<ntiles, 1024, 0, stream>>>(count, ncell, tiles, start, open);
+        rdf_place_kernel<<<blocks, kThreads, 0, stream>>>(N, p4, cell_of, rank, start, sorted);
+        rdf_cells_kernel<<<blocks, kThreads, shm, stream>>>(N, sorted, g, start, pp, rmax2, inv_dr, nbins, hist);
+    }
+    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}

@@ -92,6 +92,7 @@ SIGNATURES = {
     "lj_gpu_synchronize": (ctypes.c_int, [P]),
     "lj_gpu_step_timed": (ctypes.c_int, [P, ctypes.c_int, P]),
     "lj_gpu_fma_peaks": (ctypes.c_int, [ctypes.c_int, P, P]),
+    "lj_gpu_rdf_noalloc": (ctypes.c_int, [P, ctypes.c_int, P, ctypes.c_int, ctypes.c_double, P, P]),
     "lj_initial_condition": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                             ctypes.c_uint, P, P, P]),
 }
