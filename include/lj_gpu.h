@@ -221,6 +221,57 @@ int lj_gpu_rdf_noalloc(const double* pos, int N, const double* box, int nbins, d
 int lj_initial_condition(int N, double temperature, double density, unsigned seed, double* x, double* v,
                          double* side);
 
+/* ------------------------------------------------------------------------
+ * Whole simulations: api::Simulation::run (api/simulation.cpp:72-117) with the
+ * control protocol of control::SimulationController
+ * (control/simulation_controller.cpp:39-146), the equilibration and
+ * observation phases (control/simulation_phase.cpp:40-135), the analyzers
+ * (physics/analyzers.cpp:44-159) and the four output files in the formats of
+ * output/sinks.cpp:40-204.  Fields mirror api::Configuration
+ * (api/configuration.hpp:35-102).
+ * ------------------------------------------------------------------------ */
+typedef struct lj_sim_config {
+    double temperature, density;
+    int particle_count;
+    unsigned random_seed;
+    double cutoff_distance, time_delta;
+    const char* eq_name;
+    double eq_tolerance;
+    int eq_sample_size, eq_adjustment_interval, eq_steady_state_time, eq_timeout;
+    const char* ob_name;
+    double ob_tolerance;
+    int ob_sample_size, ob_observation_interval, ob_observation_count;
+    const char* event_log;
+    const char* thermodynamic_log;
+    const char* observation_log;
+    const char* snapshot_log;
+    int precision;  /* LJ_PRECISION_* */
+    int device;
+} lj_sim_config;
+
+typedef struct lj_sim_result {
+    long long time_steps;
+    int outcome;       /* 0 completed, 1 aborted in equilibration, 2 aborted in observation */
+    int observations;
+    double seconds;
+} lj_sim_result;
+
+/* Run one simulation to completion, writing the four files; echo != 0 also
+ * prints each event line to stdout as it happens (SimulationBuffer,
+ * api/simulation_buffer.cpp:35-58).  Thread-safe across distinct calls (each
+ * owns its context), as the reference's SimulationPool runs one per thread. */
+int lj_sim_run(const lj_sim_config* cfg, int echo, lj_sim_result* result);
+
+/* The number format of the CSV files (fmt's "{}" for a double, as used by
+ * output/sinks.cpp:116-204): shortest round-trip digits, fixed notation for
+ * decimal exponents in [-4, 16), otherwise d.ddde+XX.  Writes a NUL-terminated
+ * string of at most cap bytes. */
+int lj_format_double(double v, char* out, int cap);
+
+/* ShortRangeForce::potential / virial / force along z (physics/forces.hpp:80-84)
+ * of physics::LennardJonesForce: out = {V, W, F_z} at separation r (host only). */
+int lj_pair_along_z(double cutoff, double r, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -35,6 +35,7 @@ struct Scalars {
     int max_count;                 // largest neighbour count at the last build
     long long builds;              // neighbour-list builds so far
     long long steps;
+    long long graph_rebuilds;      // rebuild subgraphs executed by step graphs
 };
 
 // Physical constants of the pair kernel.

@@ -74,7 +74,15 @@ struct lj_ctx {
     int* dbg_cell_of = nullptr;
     int* dbg_tiles = nullptr;
 
-    long long launches = 0;
+    long long launches = 0;       // kernels launched directly (gated-off ones included)
+    long long host_steps = 0;     // mirror of the device step counter
+    // step graphs: kick_drift -> decide -> IF(rebuild chain) -> force -> finalize, unrolled
+    cudaStream_t side = nullptr;  // captures the conditional body
+    cudaGraphExec_t graph_k = nullptr;
+    int graph_steps = 0;          // steps per graph launch (0: graphs unavailable)
+    bool graph_tried = false;
+    long long graph_launched_steps = 0;
+    int rebuild_kernels = 0;      // kernels in one rebuild chain
     char err[512] = {0};
 };
 
@@ -164,7 +172,7 @@ int launch_rebuild(lj_ctx* ctx) {
     scatter_kernel<true><<<blocks_for(N), kThreads, 0, ctx->stream>>>(N, ctx->cell_of, ctx->rank,
                                                                         ctx->start, ctx->order, gate);
     CKL();
-    cell_sort_kernel<true><<<blocks_for(ctx->list_grid.ncell()), kThreads, 0, ctx->stream>>>(
+    cell_sort_kernel<true><<<blocks_for(ctx->list_grid.ncell(), kSortWarps), 32 * kSortWarps, 0, ctx->stream>>>(
         ctx->list_grid.ncell(), ctx->start, ctx->order, gate);
     CKL();
     gather_kernel<<<blocks_for(N), kThreads, 0, ctx->stream>>>(
@@ -185,7 +193,7 @@ int launch_rebuild(lj_ctx* ctx) {
         build_list_kernel<true><<<blocks_for(N), kThreads, 0, ctx->stream>>>(
             N, ctx->pos, ctx->posf, ctx->list_grid, ctx->start, Lf, cut2, ctx->cap, ctx->nbr, ctx->cnt, ctx->sc, gate);
     else
-        build_list_kernel<false><<<blocks_for(N), kThreads, 0, ctx->stream>>>(
+        build_list_warp_kernel<<<blocks_for(ctx->list_grid.ncell(), kBuildWarps), 32 * kBuildWarps, 0, ctx->stream>>>(
             N, ctx->pos, ctx->posf, ctx->list_grid, ctx->start, Lf, cut2, ctx->cap, ctx->nbr, ctx->cnt, ctx->sc, gate);
     CKL();
     if (ctx->p.precision == LJ_PRECISION_MIXED) {
@@ -232,25 +240,21 @@ int launch_force(lj_ctx* ctx, bool kick) {
 int launch_kick_drift(lj_ctx* ctx) {
     int N = ctx->N;
     bool track = !ctx->rebuild_always && ctx->p.force_kind != LJ_FORCE_NONE;
+    bool local = ctx->p.precision == LJ_PRECISION_MIXED && ctx->p.force_kind == LJ_FORCE_LJ && !ctx->small_box;
     Soa s = soa_of(ctx->soa, N);
     dim3 gr(ctx->nblocks), bl(kThreads);
-    if (ctx->p.periodic) {
-        if (track) kick_drift_kernel<true, true><<<gr, bl, 0, ctx->stream>>>(N, ctx->pos, s, ctx->bd, ctx->pp, ctx->sc);
-        else kick_drift_kernel<true, false><<<gr, bl, 0, ctx->stream>>>(N, ctx->pos, s, ctx->bd, ctx->pp, ctx->sc);
-    } else {
-        kick_drift_kernel<false, false><<<gr, bl, 0, ctx->stream>>>(N, ctx->pos, s, ctx->bd, ctx->pp, ctx->sc);
-    }
+#define LJ_KD(P, T, Lc) \
+    kick_drift_kernel<P, T, Lc><<<gr, bl, 0, ctx->stream>>>(N, ctx->pos, s, ctx->bd, ctx->bx, ctx->posl, ctx->pp, ctx->sc)
+    if (!ctx->p.periodic) LJ_KD(false, false, false);
+    else if (local) { if (track) LJ_KD(true, true, true); else LJ_KD(true, false, true); }
+    else { if (track) LJ_KD(true, true, false); else LJ_KD(true, false, false); }
+#undef LJ_KD
     CKL();
-    if (ctx->p.precision == LJ_PRECISION_MIXED && ctx->p.force_kind == LJ_FORCE_LJ && !ctx->small_box) {
-        mixed_update_local_kernel<<<gr, bl, 0, ctx->stream>>>(N, s, ctx->bd, ctx->bx, ctx->list_grid,
-                                                              ctx->posl);
-        CKL();
-    }
     return LJ_OK;
 }
 
-// One velocity-Verlet step writing its record to ring slot `slot`.
-int launch_step(lj_ctx* ctx, int slot) {
+// One velocity-Verlet step; its record goes to ring slot (step index mod ring_cap).
+int launch_step(lj_ctx* ctx) {
     int rc = launch_kick_drift(ctx);
     if (rc) return rc;
     bool forces = ctx->p.force_kind != LJ_FORCE_NONE;
@@ -265,8 +269,126 @@ int launch_step(lj_ctx* ctx, int slot) {
         CKL();
     }
     finalize_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->partials, ctx->nblocks, ctx->N, ctx->pp.dt, 0,
-                                                 forces ? 1 : 0, ctx->sc, ctx->ring + 7 * (size_t)slot);
+                                                 forces ? 1 : 0, ctx->sc, ctx->ring, ctx->ring_cap);
     CKL();
+    return LJ_OK;
+}
+
+// Capture `nsteps` steps into one executable graph.  Each step is
+//   kick_drift -> decide -> IF(rebuild chain) -> force(+kick) -> finalize
+// where `decide` sets the conditional from the device-side gate, so the
+// rebuild kernels are not even launched on the steps that do not need them.
+// Returns LJ_OK with ctx->graph_k set, or an error (the caller then keeps
+// launching the steps one kernel at a time).
+int build_step_graph(lj_ctx* ctx, int nsteps) {
+    cudaStream_t main = ctx->stream;
+    long long launches0 = ctx->launches;
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(main, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return set_err(ctx, LJ_ERR_CUDA, cudaGetErrorString(e));
+    int rc = LJ_OK;
+    bool forces = ctx->p.force_kind != LJ_FORCE_NONE;
+    for (int st = 0; st < nsteps && rc == LJ_OK; ++st) {
+        rc = launch_kick_drift(ctx);
+        if (rc) break;
+        if (forces) {
+            cudaStreamCaptureStatus cs;
+            cudaGraph_t g = nullptr;
+            const cudaGraphNode_t* deps = nullptr;
+            size_t ndeps = 0;
+            cudaGraphConditionalHandle h;
+            if ((e = cudaStreamGetCaptureInfo(main, &cs, nullptr, &g, &deps, &ndeps)) != cudaSuccess ||
+                (e = cudaGraphConditionalHandleCreate(&h, g, 0, 0)) != cudaSuccess) {
+                rc = LJ_ERR_CUDA;
+                break;
+            }
+            decide_rebuild_kernel<<<1, 1, 0, main>>>(gate_of(ctx), h, ctx->sc);
+            if ((e = cudaGetLastError()) != cudaSuccess ||
+                (e = cudaStreamGetCaptureInfo(main, &cs, nullptr, &g, &deps, &ndeps)) != cudaSuccess) {
+                rc = LJ_ERR_CUDA;
+                break;
+            }
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = h;
+            cp.conditional.type = cudaGraphCondTypeIf;
+            cp.conditional.size = 1;
+            cudaGraphNode_t cnode;
+            if ((e = cudaGraphAddNode(&cnode, g, deps, ndeps, &cp)) != cudaSuccess ||
+                (e = cudaStreamUpdateCaptureDependencies(main, &cnode, 1, cudaStreamSetCaptureDependencies)) !=
+                    cudaSuccess) {
+                rc = LJ_ERR_CUDA;
+                break;
+            }
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            if ((e = cudaStreamBeginCaptureToGraph(ctx->side, body, nullptr, nullptr, 0,
+                                                   cudaStreamCaptureModeThreadLocal)) != cudaSuccess) {
+                rc = LJ_ERR_CUDA;
+                break;
+            }
+            long long l0 = ctx->launches;
+            ctx->stream = ctx->side;
+            rc = launch_rebuild(ctx);
+            ctx->stream = main;
+            ctx->rebuild_kernels = (int)(ctx->launches - l0);
+            cudaGraph_t body_out = nullptr;
+            cudaError_t e2 = cudaStreamEndCapture(ctx->side, &body_out);
+            if (rc == LJ_OK && e2 != cudaSuccess) {
+                e = e2;
+                rc = LJ_ERR_CUDA;
+            }
+            if (rc) break;
+            rc = launch_force(ctx, true);
+        } else {
+            kick_measure_kernel<<<ctx->nblocks, kThreads, 0, main>>>(ctx->N, soa_of(ctx->soa, ctx->N), ctx->pp.dt, 1,
+                                                                     ctx->partials);
+            if (cudaGetLastError() != cudaSuccess) rc = LJ_ERR_CUDA;
+        }
+        if (rc) break;
+        finalize_kernel<<<1, 1024, 0, main>>>(ctx->partials, ctx->nblocks, ctx->N, ctx->pp.dt, 0, forces ? 1 : 0,
+                                              ctx->sc, ctx->ring, ctx->ring_cap);
+        if (cudaGetLastError() != cudaSuccess) rc = LJ_ERR_CUDA;
+    }
+    ctx->stream = main;
+    cudaError_t ee = cudaStreamEndCapture(main, &graph);
+    ctx->launches = launches0;  // captured launches are not executions
+    if (rc == LJ_OK && ee != cudaSuccess) {
+        e = ee;
+        rc = LJ_ERR_CUDA;
+    }
+    if (rc == LJ_OK) {
+        e = cudaGraphInstantiate(&ctx->graph_k, graph, 0);
+        if (e != cudaSuccess) rc = LJ_ERR_CUDA;
+    }
+    if (graph) cudaGraphDestroy(graph);
+    if (rc) {
+        ctx->graph_k = nullptr;
+        std::snprintf(ctx->err, sizeof ctx->err, "step graph unavailable: %s", cudaGetErrorString(e));
+        cudaGetLastError();  // clear the sticky-free error state of the failed capture
+    }
+    return rc;
+}
+
+constexpr int kGraphSteps = 8;
+
+// Enqueue nsteps steps: whole step graphs where available, single launches for the rest.
+int enqueue_steps(lj_ctx* ctx, int nsteps) {
+    if (!ctx->graph_tried) {
+        ctx->graph_tried = true;
+        if (build_step_graph(ctx, kGraphSteps) == LJ_OK) ctx->graph_steps = kGraphSteps;
+    }
+    int s = 0;
+    if (ctx->graph_steps > 0) {
+        for (; s + ctx->graph_steps <= nsteps; s += ctx->graph_steps) {
+            CK(cudaGraphLaunch(ctx->graph_k, ctx->stream));
+            ctx->graph_launched_steps += ctx->graph_steps;
+        }
+    }
+    for (; s < nsteps; ++s) {
+        int rc = launch_step(ctx);
+        if (rc) return rc;
+    }
+    ctx->host_steps += nsteps;
     return LJ_OK;
 }
 
@@ -287,6 +409,8 @@ void free_all(lj_ctx* c) {
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (c->host_ring) cudaFreeHost(c->host_ring);
+    if (c->graph_k) cudaGraphExecDestroy(c->graph_k);
+    if (c->side) cudaStreamDestroy(c->side);
     if (c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -341,6 +465,7 @@ int lj_gpu_create(const lj_params* params, lj_ctx** out) {
     int N = ctx->N = p.particle_count;
     CK(cudaSetDevice(p.device));
     CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
 
     // pair constants (lennard_jones_force.cpp:33-74)
     PairParams& pp = ctx->pp;
@@ -408,7 +533,7 @@ int lj_gpu_create(const lj_params* params, lj_ctx** out) {
     CK(cudaMalloc(&ctx->partials, sizeof(double) * 4 * ctx->nblocks));
     CK(cudaMalloc(&ctx->sc, sizeof(Scalars)));
     ctx->ring_cap = 1024;
-    CK(cudaMalloc(&ctx->ring, sizeof(double) * 7 * ctx->ring_cap));
+    CK(cudaMalloc(&ctx->ring, sizeof(double) * 7 * (ctx->ring_cap + 1)));
     CK(cudaMalloc(&ctx->dscratch, sizeof(double) * 8));
     ctx->dL = ctx->dscratch + 4;
     CK(cudaMallocHost(&ctx->host_ring, sizeof(double) * 7 * ctx->ring_cap));
@@ -529,7 +654,7 @@ int lj_gpu_compute_forces(lj_ctx* ctx, double* pe, double* virial) {
         rc = launch_force(ctx, false);
         if (rc) return rc;
         finalize_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->partials, ctx->nblocks, ctx->N, ctx->pp.dt, 1, 1,
-                                                     ctx->sc, ctx->ring);
+                                                     ctx->sc, ctx->ring, ctx->ring_cap);
         CKL();
     }
     int rc = read_flags(ctx);
@@ -548,15 +673,20 @@ int lj_gpu_step(lj_ctx* ctx, int nsteps, lj_thermo* out) {
     int done = 0;
     while (done < nsteps) {
         int chunk = std::min(nsteps - done, ctx->ring_cap);
-        for (int s = 0; s < chunk; ++s) {
-            int rc = launch_step(ctx, s);
-            if (rc) return rc;
-        }
+        long long first = ctx->host_steps;
+        int rc = enqueue_steps(ctx, chunk);
+        if (rc) return rc;
         if (out) {
-            CK(cudaMemcpyAsync(ctx->host_ring, ctx->ring, sizeof(double) * 7 * chunk, cudaMemcpyDeviceToHost,
-                               ctx->stream));
+            // records of steps first .. first+chunk-1 sit at ring slots (step mod ring_cap)
+            int s0 = (int)(first % ctx->ring_cap);
+            int n1 = std::min(chunk, ctx->ring_cap - s0);
+            CK(cudaMemcpyAsync(ctx->host_ring, ctx->ring + 7 * (size_t)s0, sizeof(double) * 7 * n1,
+                               cudaMemcpyDeviceToHost, ctx->stream));
+            if (n1 < chunk)
+                CK(cudaMemcpyAsync(ctx->host_ring + 7 * (size_t)n1, ctx->ring, sizeof(double) * 7 * (chunk - n1),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
         }
-        int rc = read_flags(ctx);  // synchronises
+        rc = read_flags(ctx);  // synchronises
         if (rc) return rc;
         if (out) std::memcpy(out + done, ctx->host_ring, sizeof(double) * 7 * chunk);
         done += chunk;
@@ -571,9 +701,10 @@ int lj_gpu_measure(lj_ctx* ctx, lj_thermo* out) {
                                                                      ctx->partials);
     CKL();
     finalize_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->partials, ctx->nblocks, ctx->N, ctx->pp.dt, 2, 0,
-                                                 ctx->sc, ctx->ring);
+                                                 ctx->sc, ctx->ring, ctx->ring_cap);
     CKL();
-    CK(cudaMemcpyAsync(ctx->host_ring, ctx->ring, sizeof(double) * 7, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->host_ring, ctx->ring + 7 * (size_t)ctx->ring_cap, sizeof(double) * 7,
+                       cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     std::memcpy(out, ctx->host_ring, sizeof(double) * 7);
     return LJ_OK;
@@ -697,7 +828,9 @@ int lj_gpu_get_stats(const lj_ctx* ctx_c, lj_stats* out) {
     out->max_neighbors = h.max_count;
     out->small_box = ctx->small_box ? 1 : 0;
     out->skin = ctx->skin;
-    out->kernel_launches = ctx->launches;
+    // direct launches + kernel nodes executed by step graphs (kick, decide, force,
+    // finalize per step, and the rebuild chain each time the conditional opened)
+    out->kernel_launches = ctx->launches + 4 * ctx->graph_launched_steps + (long long)ctx->rebuild_kernels * h.graph_rebuilds;
     return LJ_OK;
 }
 
@@ -718,11 +851,7 @@ void* lj_gpu_stream(lj_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 int lj_gpu_step_async(lj_ctx* ctx, int nsteps) {
     if (!ctx || nsteps < 0) return set_err(ctx, LJ_ERR_ARG, "bad step arguments");
     CK(cudaSetDevice(ctx->p.device));
-    for (int s = 0; s < nsteps; ++s) {
-        int rc = launch_step(ctx, s % ctx->ring_cap);
-        if (rc) return rc;
-    }
-    return LJ_OK;
+    return enqueue_steps(ctx, nsteps);
 }
 
 int lj_gpu_synchronize(lj_ctx* ctx) {
@@ -741,7 +870,7 @@ int lj_gpu_step_timed(lj_ctx* ctx, int nsteps, lj_phase_times* out) {
     CK(cudaMemcpy(&before, ctx->sc, sizeof before, cudaMemcpyDeviceToHost));
     bool forces = ctx->p.force_kind != LJ_FORCE_NONE;
     for (int s = 0; s < nsteps; ++s) {
-        int slot = s % ctx->ring_cap, rc;
+        int rc;
         CK(cudaEventRecord(ev[0], ctx->stream));
         if ((rc = launch_kick_drift(ctx))) return rc;
         CK(cudaEventRecord(ev[1], ctx->stream));
@@ -756,7 +885,7 @@ int lj_gpu_step_timed(lj_ctx* ctx, int nsteps, lj_phase_times* out) {
         }
         CK(cudaEventRecord(ev[3], ctx->stream));
         finalize_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->partials, ctx->nblocks, ctx->N, ctx->pp.dt, 0,
-                                                     forces ? 1 : 0, ctx->sc, ctx->ring + 7 * (size_t)slot);
+                                                     forces ? 1 : 0, ctx->sc, ctx->ring, ctx->ring_cap);
         CKL();
         CK(cudaEventRecord(ev[4], ctx->stream));
         CK(cudaEventSynchronize(ev[4]));
@@ -772,6 +901,7 @@ int lj_gpu_step_timed(lj_ctx* ctx, int nsteps, lj_phase_times* out) {
     CK(cudaMemcpy(&after, ctx->sc, sizeof after, cudaMemcpyDeviceToHost));
     out->steps = nsteps;
     out->rebuilds = after.builds - before.builds;
+    ctx->host_steps += nsteps;
     return read_flags(ctx);
 }
 

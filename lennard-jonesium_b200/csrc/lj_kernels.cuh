@@ -38,15 +38,16 @@ struct Gate {
 // ---------------------------------------------------------------------------
 // Integration: integrator.cpp:62-88, first half (kick, drift, displacement, wrap)
 // ---------------------------------------------------------------------------
-template <bool PERIODIC, bool TRACK>
+template <bool PERIODIC, bool TRACK, bool LOCAL>
 static __global__ void __launch_bounds__(kThreads)
 kick_drift_kernel(int N, double4* __restrict__ pos, Soa s, const double* __restrict__ bd,
-                  PairParams pp, Scalars* sc) {
+                  const double* __restrict__ bx, float4* __restrict__ posl, PairParams pp, Scalars* sc) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double m = 0.0;
     if (i < N) {
         double4 x = pos[i];
         double xs[3] = {x.x, x.y, x.z};
+        float l[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             double v = kick(s.at(VX + k, i), s.at(FX + k, i), pp.dt);
@@ -57,12 +58,15 @@ kick_drift_kernel(int N, double4* __restrict__ pos, Soa s, const double* __restr
             s.at(VX + k, i) = v;
             s.at(DX + k, i) = dn;
             xs[k] = xn;
-            if (TRACK) {
+            if (TRACK || LOCAL) {
                 double e = dn - bd[(size_t)k * N + i];
                 m = fma(e, e, m);
+                // mixed path: cell-local FP32 coordinate xl = bx + (d - d_build)
+                if (LOCAL) l[k] = (float)(bx[(size_t)k * N + i] + e);
             }
         }
         pos[i] = make_double4(xs[0], xs[1], xs[2], 0.0);
+        if (LOCAL) posl[i] = make_float4(l[0], l[1], l[2], 0.f);
     }
     if (TRACK) {
         m = warp_max(m);
@@ -176,22 +180,41 @@ scatter_kernel(int N, const int* __restrict__ cell_of, const int* __restrict__ r
 // sort, so the order is a fixed function of the trajectory and every run is
 // bit-reproducible without reading atom ids.  (The reference's own cell
 // contents, ascending atom id, are produced by lj_gpu_debug_cells.)
+// One warp per cell: cells of up to 32 atoms are sorted in registers by a
+// bitonic network over warp shuffles; larger cells (rare) by one lane.
+constexpr int kSortWarps = 4;
+
 template <bool GATED>
-static __global__ void __launch_bounds__(kThreads)
+static __global__ void __launch_bounds__(32 * kSortWarps)
 cell_sort_kernel(int ncell, const int* __restrict__ start, int* __restrict__ order, Gate gate) {
     if (GATED && !gate.open()) return;
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    int lane = threadIdx.x & 31;
+    int c = blockIdx.x * kSortWarps + (threadIdx.x >> 5);
     if (c >= ncell) return;
-    int b = start[c], e = start[c + 1];
-    for (int k = b + 1; k < e; ++k) {
-        int v = order[k];
-        int q = k - 1;
-        while (q >= b && order[q] > v) {
-            order[q + 1] = order[q];
-            --q;
-        }
-        order[q + 1] = v;
+    int b = start[c], e = start[c + 1], n = e - b;
+    if (n <= 1) return;
+    if (n <= 32) {
+        int v = lane < n ? order[b + lane] : 0x7fffffff;
+#pragma unroll
+        for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                int o = __shfl_xor_sync(0xffffffffu, v, j);
+                bool up = (lane & k) == 0, lower = (lane & j) == 0;
+                v = (lower == up) ? min(v, o) : max(v, o);
+            }
+        if (lane < n) order[b + lane] = v;
+        return;
     }
+    if (lane == 0)
+        for (int k = b + 1; k < e; ++k) {
+            int v = order[k], q = k - 1;
+            while (q >= b && order[q] > v) {
+                order[q + 1] = order[q];
+                --q;
+            }
+            order[q + 1] = v;
+        }
 }
 
 // Gather the state into sorted order (into the scratch copies).
@@ -294,6 +317,116 @@ build_list_kernel(int N, const double4* __restrict__ pos, const float4* __restri
     if ((threadIdx.x & 31) == 0) {
         atomicMax(&sc->max_count, m);
         if (m > cap) atomicExch(&sc->overflow, 1);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd((unsigned long long*)&sc->builds, 1ull);
+}
+
+// Warp-per-cell list build for grids of >= 3 cells per axis (the minimum-image
+// form).  One warp owns one list cell: lanes hold the cell's atoms (in chunks of
+// 32).  For each of the 27 stencil cells the warp stages 32 candidates at a
+// time in shared memory (one coalesced load, stored negated and as separate
+// x / y / z rows), and every lane tests every staged candidate through
+// broadcast reads, two candidates per instruction with Blackwell's packed
+// FP32x2 add / multiply / fma.  The test loop only sets bits of a hit mask; a
+// short per-lane loop over the set bits then appends the entries, so the
+// append code is not issued once per candidate.  Each lane collects entries in
+// a 4-entry shared buffer and writes whole groups (one 16-byte store).
+// Entries, their order (stencil cell, then slot) and the candidate radius are
+// those of build_list_kernel<false>.
+constexpr int kBuildWarps = 4;
+
+__device__ __forceinline__ void append_entry(unsigned (&grp)[4], int& n, int cap, unsigned entry,
+                                             uint4* __restrict__ nbr4, size_t N, int i) {
+    if (n < cap) {
+        grp[n & 3] = entry;
+        if ((n & 3) == 3) nbr4[(size_t)(n >> 2) * N + i] = make_uint4(grp[0], grp[1], grp[2], grp[3]);
+    }
+    ++n;
+}
+
+static __global__ void __launch_bounds__(32 * kBuildWarps)
+build_list_warp_kernel(int N, const double4* __restrict__ pos, const float4* __restrict__ posf, Grid g,
+                       const int* __restrict__ start, float3 Lf, float cut2, int cap,
+                       uint4* __restrict__ nbr4, int* __restrict__ cnt, Scalars* sc, Gate gate) {
+    if (!gate.open()) return;
+    __shared__ __align__(16) float cxs[kBuildWarps][3][32];
+    __shared__ unsigned grp_s[kBuildWarps][32][4];
+    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int c = blockIdx.x * kBuildWarps + warp;
+    int ncell = g.ncell();
+    int wmax = 0;
+    unsigned (&grp)[4] = grp_s[warp][lane];
+    if (c < ncell) {
+        int ca = c / (g.n[1] * g.n[2]), cb = (c / g.n[2]) % g.n[1], cc = c % g.n[2];
+        int hs = start[c], he = start[c + 1];
+        for (int h0 = hs; h0 < he; h0 += 32) {
+            int i = h0 + lane;
+            bool own = i < he;
+            float4 xi = own ? posf[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+            int n = 0;
+            for (int a = -1; a <= 1; ++a) {
+                int na = ca + a, ia = na < 0 ? -1 : (na >= g.n[0] ? 1 : 0);
+                na -= ia * g.n[0];
+                for (int b = -1; b <= 1; ++b) {
+                    int nb = cb + b, ib = nb < 0 ? -1 : (nb >= g.n[1] ? 1 : 0);
+                    nb -= ib * g.n[1];
+                    for (int d = -1; d <= 1; ++d) {
+                        int nc = cc + d, ic = nc < 0 ? -1 : (nc >= g.n[2] ? 1 : 0);
+                        nc -= ic * g.n[2];
+                        int cell = g.flat(na, nb, nc);
+                        // home atom shifted by the lattice image of this stencil cell
+                        float2 sx = make_float2(xi.x - ia * Lf.x, xi.x - ia * Lf.x);
+                        float2 sy = make_float2(xi.y - ib * Lf.y, xi.y - ib * Lf.y);
+                        float2 sz = make_float2(xi.z - ic * Lf.z, xi.z - ic * Lf.z);
+                        unsigned code = (unsigned)image_code(a, b, d) << kSlotBits;
+                        int js = start[cell], je = start[cell + 1];
+                        for (int j0 = js; j0 < je; j0 += 32) {
+                            int cntj = min(32, je - j0);
+                            __syncwarp();
+                            float4 q = lane < cntj ? posf[j0 + lane] : make_float4(1e18f, 1e18f, 1e18f, 0.f);
+                            cxs[warp][0][lane] = -q.x;
+                            cxs[warp][1][lane] = -q.y;
+                            cxs[warp][2][lane] = -q.z;
+                            __syncwarp();
+                            unsigned mask = 0;
+                            for (int t = 0; t < cntj; t += 2) {
+                                float2 qx = *reinterpret_cast<const float2*>(&cxs[warp][0][t]);
+                                float2 qy = *reinterpret_cast<const float2*>(&cxs[warp][1][t]);
+                                float2 qz = *reinterpret_cast<const float2*>(&cxs[warp][2][t]);
+                                float2 dx = __fadd2_rn(sx, qx), dy = __fadd2_rn(sy, qy), dz = __fadd2_rn(sz, qz);
+                                float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+                                mask |= (r2.x < cut2 ? 1u : 0u) << t;
+                                mask |= (r2.y < cut2 ? 2u : 0u) << t;
+                            }
+                            if (cntj < 32) mask &= (1u << cntj) - 1u;  // the odd tail reads a far-away filler
+                            unsigned self = (unsigned)(i - j0);
+                            if (self < 32u) mask &= ~(1u << self);
+                            if (!own) mask = 0;
+                            while (mask) {
+                                int t = __ffs(mask) - 1;
+                                mask &= mask - 1;
+                                append_entry(grp, n, cap, (unsigned)(j0 + t) | code, nbr4, N, i);
+                            }
+                        }
+                    }
+                }
+            }
+            if (own) {
+                int m = n < cap ? n : cap;
+                cnt[i] = m;
+                if (m & 3) {  // pad the last group with the ghost slot
+                    for (int k = m & 3; k < 4; ++k) grp[k] = (unsigned)N | (13u << kSlotBits);
+                    nbr4[(size_t)(m >> 2) * N + i] = make_uint4(grp[0], grp[1], grp[2], grp[3]);
+                }
+                wmax = max(wmax, n);
+            }
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) wmax = max(wmax, __shfl_down_sync(0xffffffffu, wmax, off));
+    if (lane == 0 && c < ncell) {
+        atomicMax(&sc->max_count, wmax);
+        if (wmax > cap) atomicExch(&sc->overflow, 1);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd((unsigned long long*)&sc->builds, 1ull);
 }
@@ -428,7 +561,7 @@ force_fp64_kernel(int N, const double4* __restrict__ pos, Soa s, const uint4* __
 // ---------------------------------------------------------------------------
 static __global__ void __launch_bounds__(1024)
 finalize_kernel(const double* __restrict__ partials, int nblocks, int N, double dt, int mode,
-                int forces_valid, Scalars* sc, double* __restrict__ out /* 7 doubles */) {
+                int forces_valid, Scalars* sc, double* __restrict__ ring, int ring_cap) {
     double acc[4] = {0, 0, 0, 0};
     for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
 #pragma unroll
@@ -439,6 +572,9 @@ finalize_kernel(const double* __restrict__ partials, int nblocks, int N, double 
             sc->pe = 0.5 * acc[1];
             sc->vir = 0.5 * acc[2];
         }
+        // a step's record goes to ring slot (step index mod ring_cap); the extra
+        // slot ring_cap holds single measurements
+        double* out = ring + 7 * (size_t)(mode == 0 ? (int)(sc->steps % ring_cap) : ring_cap);
         if (mode == 0) {
             sc->t = sc->t + dt;  // integrator.cpp:85
             sc->steps += 1;
@@ -461,6 +597,13 @@ finalize_kernel(const double* __restrict__ partials, int nblocks, int N, double 
         sc->max_disp2 = 0ull;
         sc->need_rebuild = 0;
     }
+}
+
+// Graph step: decide on the device whether the rebuild subgraph runs this step.
+static __global__ void decide_rebuild_kernel(Gate gate, cudaGraphConditionalHandle h, Scalars* sc) {
+    bool open = gate.open();
+    if (open) sc->graph_rebuilds += 1;
+    cudaGraphSetConditional(h, open ? 1u : 0u);
 }
 
 static __global__ void __launch_bounds__(kThreads)

@@ -62,19 +62,6 @@ mixed_build_local_kernel(int N, const double4* __restrict__ pos, Soa s, Grid g, 
     posl[i] = make_float4(l[0], l[1], l[2], 0.f);
 }
 
-// Every step after the drift: xl = bx + (d - d_build).
-static __global__ void __launch_bounds__(kThreads)
-mixed_update_local_kernel(int N, Soa s, const double* __restrict__ bd, const double* __restrict__ bx,
-                          Grid g, float4* __restrict__ posl) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
-    float l[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k)
-        l[k] = (float)(bx[(size_t)k * N + i] + (s.at(DX + k, i) - bd[(size_t)k * N + i]));
-    posl[i] = make_float4(l[0], l[1], l[2], 0.f);
-}
-
 __device__ __forceinline__ float rcp_approx(float x) {
     float y;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));

@@ -57,6 +57,28 @@ class PhaseTimes(ctypes.Structure):
                 ("steps", ctypes.c_longlong), ("rebuilds", ctypes.c_longlong)]
 
 
+class SimConfig(ctypes.Structure):
+    _fields_ = [
+        ("temperature", ctypes.c_double), ("density", ctypes.c_double),
+        ("particle_count", ctypes.c_int), ("random_seed", ctypes.c_uint),
+        ("cutoff_distance", ctypes.c_double), ("time_delta", ctypes.c_double),
+        ("eq_name", ctypes.c_char_p), ("eq_tolerance", ctypes.c_double),
+        ("eq_sample_size", ctypes.c_int), ("eq_adjustment_interval", ctypes.c_int),
+        ("eq_steady_state_time", ctypes.c_int), ("eq_timeout", ctypes.c_int),
+        ("ob_name", ctypes.c_char_p), ("ob_tolerance", ctypes.c_double),
+        ("ob_sample_size", ctypes.c_int), ("ob_observation_interval", ctypes.c_int),
+        ("ob_observation_count", ctypes.c_int),
+        ("event_log", ctypes.c_char_p), ("thermodynamic_log", ctypes.c_char_p),
+        ("observation_log", ctypes.c_char_p), ("snapshot_log", ctypes.c_char_p),
+        ("precision", ctypes.c_int), ("device", ctypes.c_int),
+    ]
+
+
+class SimResult(ctypes.Structure):
+    _fields_ = [("time_steps", ctypes.c_longlong), ("outcome", ctypes.c_int),
+                ("observations", ctypes.c_int), ("seconds", ctypes.c_double)]
+
+
 class LJError(RuntimeError):
     """A C-ABI call returned a non-zero status."""
 
@@ -93,6 +115,9 @@ SIGNATURES = {
     "lj_gpu_step_timed": (ctypes.c_int, [P, ctypes.c_int, P]),
     "lj_gpu_fma_peaks": (ctypes.c_int, [ctypes.c_int, P, P]),
     "lj_gpu_rdf_noalloc": (ctypes.c_int, [P, ctypes.c_int, P, ctypes.c_int, ctypes.c_double, P, P]),
+    "lj_sim_run": (ctypes.c_int, [P, ctypes.c_int, P]),
+    "lj_format_double": (ctypes.c_int, [ctypes.c_double, ctypes.c_char_p, ctypes.c_int]),
+    "lj_pair_along_z": (ctypes.c_int, [ctypes.c_double, ctypes.c_double, P]),
     "lj_initial_condition": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                             ctypes.c_uint, P, P, P]),
 }
