@@ -262,6 +262,13 @@ typedef struct lj_sim_result {
  * owns its context), as the reference's SimulationPool runs one per thread. */
 int lj_sim_run(const lj_sim_config* cfg, int echo, lj_sim_result* result);
 
+/* A whole sweep on one batched engine (lj_batch_*): n configurations sharing
+ * cutoff and time step, each with its own control protocol and four files,
+ * all systems stepping together in chunks that end at the earliest step at
+ * which any running simulation can act.  results (may be NULL) receives n
+ * entries.  The batched form of run_sweep. */
+int lj_sim_run_batch(const lj_sim_config* cfgs, int n, int echo, lj_sim_result* results);
+
 /* The number format of the CSV files (fmt's "{}" for a double, as used by
  * output/sinks.cpp:116-204): shortest round-trip digits, fixed notation for
  * decimal exponents in [-4, 16), otherwise d.ddde+XX.  Writes a NUL-terminated
@@ -271,6 +278,44 @@ int lj_format_double(double v, char* out, int cap);
 /* ShortRangeForce::potential / virial / force along z (physics/forces.hpp:80-84)
  * of physics::LennardJonesForce: out = {V, W, F_z} at separation r (host only). */
 int lj_pair_along_z(double cutoff, double r, double* out);
+
+/* ------------------------------------------------------------------------
+ * Batched systems: many independent systems of uneven size advanced together,
+ * one kernel launch (and one CUDA graph per chunk of steps) for all of them,
+ * over a packed system table.  Replaces, for a sweep, the reference's
+ * SimulationPool of one-simulation-per-thread workers
+ * (api/simulation_pool.cpp:35-101) driven by run_sweep
+ * (src/python/lennardjonesium/orchestration/run_sweep.py:37-139).  Each system
+ * evolves exactly as it would alone through lj_gpu_* (FP64, LJ force,
+ * periodic); every box edge must be at least 3 * cutoff.
+ * ------------------------------------------------------------------------ */
+typedef struct lj_batch_system {
+    int particle_count;
+    double box[3];
+    double time_delta;
+    double skin;  /* < 0: the default rule of lj_gpu_create */
+} lj_batch_system;
+
+typedef struct lj_batch lj_batch;
+
+int lj_batch_create(const lj_batch_system* systems, int nsys, double cutoff, int device, lj_batch** out);
+int lj_batch_destroy(lj_batch* batch);
+const char* lj_batch_last_error(const lj_batch* batch);
+/* Replace one system's state: positions and velocities (N x stride doubles,
+ * v may be NULL); displacements, forces, time and energies restart at zero. */
+int lj_batch_upload_system(lj_batch* batch, int sys, const double* x, const double* v, int stride);
+int lj_batch_download_system(lj_batch* batch, int sys, double* x, double* v, double* F, int stride);
+/* An inactive system is frozen: its atoms are not integrated and it takes no steps. */
+int lj_batch_set_active(lj_batch* batch, int sys, int active);
+/* nsteps steps of every active system; out (may be NULL) receives nsteps x nsys
+ * records, step-major (inactive systems' entries are not written). */
+int lj_batch_step(lj_batch* batch, int nsteps, lj_thermo* out);
+/* Instantaneous measurement of every system: out receives nsys records. */
+int lj_batch_measure(lj_batch* batch, lj_thermo* out);
+/* physics::set_temperature for one system (transformations.cpp:94-116). */
+int lj_batch_set_temperature(lj_batch* batch, int sys, double target, double* measured);
+/* Totals for tests and tuning: atoms, neighbour-list builds per system, direct kernel launches. */
+int lj_batch_info(const lj_batch* batch, int* total_atoms, long long* builds_per_system, long long* kernel_launches);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,982 @@
+// lj_batch.cu -- many independent systems of uneven size in one launch per
+// kernel: the batched engine behind run_sweep (a grid of (T, rho) runs).
+//
+// Packed system table.  The atoms of all systems are concatenated (system s
+// owns slots [atom_off_s, atom_off_s + N_s)), and so are their list-cell grids
+// (cells [cell_off_s, cell_off_s + ncell_s)).  Each per-atom kernel runs over a
+// block table in which every block belongs to one system and covers the same
+// 128 atoms as block j of that system run alone; every cell belongs to one
+// system.  Rebuilds are gated per system by its own skin criterion, the cell
+// scan is segmented per system, and each system's records come from its own
+// blocks' partial sums in the single-system order.  A batched run therefore
+// reproduces, bit for bit, the same systems run one at a time through
+// lj_gpu_* (tests/test_gpu_batch.py checks this).
+//
+// One step = kick_drift -> decide (per-system rebuild flags + graph conditional)
+// -> IF(rebuild chain) -> force(+kick) -> finalize (one block per system), and
+// lj_batch_step launches whole CUDA graphs of several such steps.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/lj_gpu.h"
+#include "lj_kernels.cuh"
+
+using namespace ljb;
+
+double list_skin(double requested, double Lmin, double rc);
+
+namespace {
+
+struct SysDev {
+    int atom_off, natoms;
+    int cell_off, ncell;
+    int blk_off, nblk;
+    Grid grid;
+    PairParams pp;
+    double thresh2;  // rebuild when max |d - d_build|^2 exceeds this
+    int always;      // zero skin: rebuild every step
+    float cut2;      // FP32 list radius^2 (widened past FP32 rounding)
+    float3 Lf;
+};
+
+struct SysState {
+    double t, pe, vir;
+    unsigned long long max_disp2;
+    int need_rebuild;
+    int rebuild;  // decided for this step
+    int active;
+    int pad;
+    long long builds, steps;
+};
+
+struct BatchFlags {
+    int overflow, nonfinite, any_rebuild, slot;  // slot: ring slot of the current step
+    long long graph_rebuilds;
+    long long step_count;                        // steps taken by the batch
+};
+
+__device__ __forceinline__ bool sys_rebuild(const SysState* st, int s) { return st[s].rebuild != 0; }
+
+// ---- integration -----------------------------------------------------------
+static __global__ void __launch_bounds__(kThreads)
+b_kick_drift_kernel(const int* __restrict__ blk_sys, const int* __restrict__ blk_first, const SysDev* __restrict__ sys,
+                    SysState* st, int Ntot, double4* __restrict__ pos, Soa s, const double* __restrict__ bd) {
+    int sidx = blk_sys[blockIdx.x];
+    const SysDev& S = sys[sidx];
+    if (!st[sidx].active) return;
+    int i = blk_first[blockIdx.x] + threadIdx.x;
+    bool own = i < S.atom_off + S.natoms;
+    double m = 0.0;
+    if (own) {
+        double4 x = pos[i];
+        double xs[3] = {x.x, x.y, x.z};
+        double dt = S.pp.dt;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            double v = kick(s.at(VX + k, i), s.at(FX + k, i), dt);
+            double inc = __dmul_rn(v, dt);
+            double xn = wrap(__dadd_rn(xs[k], inc), S.pp.L[k]);
+            double dn = __dadd_rn(s.at(DX + k, i), inc);
+            s.at(VX + k, i) = v;
+            s.at(DX + k, i) = dn;
+            xs[k] = xn;
+            double e = dn - bd[(size_t)k * Ntot + i];
+            m = fma(e, e, m);
+        }
+        pos[i] = make_double4(xs[0], xs[1], xs[2], 0.0);
+    }
+    m = warp_max(m);
+    if ((threadIdx.x & 31) == 0 && m > 0.0)
+        atomicMax(&st[sidx].max_disp2, (unsigned long long)__double_as_longlong(m));
+}
+
+// Per-system rebuild decision; opens the graph conditional if any system rebuilds.
+static __global__ void b_decide_kernel(const SysDev* __restrict__ sys, SysState* st, int nsys, BatchFlags* fl,
+                                       int ring_cap, cudaGraphConditionalHandle h, int use_handle) {
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    for (int s = threadIdx.x; s < nsys; s += blockDim.x) {
+        bool r = st[s].active &&
+                 (sys[s].always || st[s].need_rebuild ||
+                  __longlong_as_double((long long)st[s].max_disp2) > sys[s].thresh2);
+        st[s].rebuild = r ? 1 : 0;
+        if (r) atomicExch(&any, 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        fl->any_rebuild = any;
+        fl->slot = (int)(fl->step_count % ring_cap);
+        fl->step_count += 1;
+        if (any) fl->graph_rebuilds += 1;
+        if (use_handle) cudaGraphSetConditional(h, any ? 1u : 0u);
+    }
+}
+
+// ---- rebuild chain (systems with st[s].rebuild only) -------------------------
+static __global__ void __launch_bounds__(kThreads)
+b_bin_kernel(const int* __restrict__ sys_of, const SysDev* __restrict__ sys, const SysState* st, int Ntot,
+             const double4* __restrict__ pos, int* __restrict__ cell_of, int* __restrict__ rank,
+             int* __restrict__ count) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= Ntot) return;
+    int s = sys_of[i];
+    if (!sys_rebuild(st, s)) return;
+    const Grid& g = sys[s].grid;
+    double4 x = pos[i];
+    int c = sys[s].cell_off + g.flat(cell_coord(x.x, g.ratio[0], g.n[0]), cell_coord(x.y, g.ratio[1], g.n[1]),
+                                     cell_coord(x.z, g.ratio[2], g.n[2]));
+    cell_of[i] = c;
+    rank[i] = atomicAdd(&count[c], 1);
+}
+
+// One block per system: exclusive scan of its cells' counts, offset by its first slot.
+static __global__ void __launch_bounds__(1024)
+b_scan_kernel(const SysDev* __restrict__ sys, const SysState* st, int* __restrict__ count, int* __restrict__ start) {
+    int s = blockIdx.x;
+    if (!sys_rebuild(st, s)) return;
+    __shared__ int tot;
+    int base = sys[s].atom_off;
+    int c0 = sys[s].cell_off, nc = sys[s].ncell;
+    for (int t0 = 0; t0 < nc; t0 += 4 * 1024) {
+        int idx = t0 + threadIdx.x * 4;
+        int c[4], sum = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            c[q] = idx + q < nc ? count[c0 + idx + q] : 0;
+            sum += c[q];
+        }
+        int ex = block_exclusive_scan<1024>(sum, &tot) + base;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (idx + q < nc) {
+                start[c0 + idx + q] = ex;
+                count[c0 + idx + q] = 0;
+            }
+            ex += c[q];
+        }
+        base += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) start[c0 + nc] = sys[s].atom_off + sys[s].natoms;
+}
+
+static __global__ void __launch_bounds__(kThreads)
+b_scatter_kernel(const int* __restrict__ sys_of, const SysState* st, int Ntot, const int* __restrict__ cell_of,
+                 const int* __restrict__ rank, const int* __restrict__ start, int* __restrict__ order) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= Ntot || !sys_rebuild(st, sys_of[i])) return;
+    order[start[cell_of[i]] + rank[i]] = i;
+}
+
+static __global__ void __launch_bounds__(32 * kSortWarps)
+b_cell_sort_kernel(const int* __restrict__ cell_sys, const SysState* st, int ncell, const int* __restrict__ start,
+                   int* __restrict__ order) {
+    int lane = threadIdx.x & 31;
+    int c = blockIdx.x * kSortWarps + (threadIdx.x >> 5);
+    if (c >= ncell || !sys_rebuild(st, cell_sys[c])) return;
+    int b = start[c], e = start[c + 1], n = e - b;
+    if (n <= 1) return;
+    if (n <= 32) {
+        int v = lane < n ? order[b + lane] : 0x7fffffff;
+#pragma unroll
+        for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                int o = __shfl_xor_sync(0xffffffffu, v, j);
+                bool up = (lane & k) == 0, lower = (lane & j) == 0;
+                v = (lower == up) ? min(v, o) : max(v, o);
+            }
+        if (lane < n) order[b + lane] = v;
+        return;
+    }
+    if (lane == 0)
+        for (int k = b + 1; k < e; ++k) {
+            int v = order[k], q = k - 1;
+            while (q >= b && order[q] > v) {
+                order[q + 1] = order[q];
+                --q;
+            }
+            order[q + 1] = v;
+        }
+}
+
+static __global__ void __launch_bounds__(kThreads)
+b_gather_kernel(const int* __restrict__ sys_of, const SysState* st, int Ntot, const int* __restrict__ order,
+                const double4* __restrict__ pos, double4* __restrict__ pos_out, Soa s, Soa s_out,
+                const int* __restrict__ ids, int* __restrict__ ids_out, double* __restrict__ bd) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= Ntot || !sys_rebuild(st, sys_of[k])) return;
+    int o = order[k];
+    pos_out[k] = pos[o];
+#pragma unroll
+    for (int f = 0; f < SOA_FIELDS; ++f) s_out.at(f, k) = s.at(f, o);
+    ids_out[k] = ids[o];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) bd[(size_t)q * Ntot + k] = s.at(DX + q, o);
+}
+
+static __global__ void __launch_bounds__(kThreads)
+b_copy_back_kernel(const int* __restrict__ sys_of, const SysState* st, int Ntot, const double4* __restrict__ pos_in,
+                   double4* __restrict__ pos, Soa s_in, Soa s, const int* __restrict__ ids_in, int* __restrict__ ids,
+                   float4* __restrict__ posf) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= Ntot || !sys_rebuild(st, sys_of[k])) return;
+    double4 x = pos_in[k];
+    pos[k] = x;
+    posf[k] = make_float4((float)x.x, (float)x.y, (float)x.z, 0.f);
+#pragma unroll
+    for (int f = 0; f < SOA_FIELDS; ++f) s.at(f, k) = s_in.at(f, k);
+    ids[k] = ids_in[k];
+}
+
+// Warp-per-cell list build (the algorithm of build_list_warp_kernel, per system).
+static __global__ void __launch_bounds__(32 * kBuildWarps)
+b_build_list_kernel(const int* __restrict__ cell_sys, const SysDev* __restrict__ sys, SysState* st, int ncell_tot,
+                    int Ntot, const float4* __restrict__ posf, const int* __restrict__ start, int cap,
+                    uint4* __restrict__ nbr4, int* __restrict__ cnt, BatchFlags* fl) {
+    __shared__ __align__(16) float cxs[kBuildWarps][3][32];
+    __shared__ unsigned grp_s[kBuildWarps][32][4];
+    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int c = blockIdx.x * kBuildWarps + warp;
+    if (c >= ncell_tot) return;
+    int sidx = cell_sys[c];
+    if (!sys_rebuild(st, sidx)) return;
+    const SysDev& S = sys[sidx];
+    const Grid& g = S.grid;
+    int lc = c - S.cell_off;
+    int ca = lc / (g.n[1] * g.n[2]), cb = (lc / g.n[2]) % g.n[1], cc = lc % g.n[2];
+    int hs = start[c], he = start[c + 1];
+    unsigned (&grp)[4] = grp_s[warp][lane];
+    int wmax = 0;
+    for (int h0 = hs; h0 < he; h0 += 32) {
+        int i = h0 + lane;
+        bool own = i < he;
+        float4 xi = own ? posf[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        int n = 0;
+        for (int a = -1; a <= 1; ++a) {
+            int na = ca + a, ia = na < 0 ? -1 : (na >= g.n[0] ? 1 : 0);
+            na -= ia * g.n[0];
+            for (int b = -1; b <= 1; ++b) {
+                int nb = cb + b, ib = nb < 0 ? -1 : (nb >= g.n[1] ? 1 : 0);
+                nb -= ib * g.n[1];
+                for (int d = -1; d <= 1; ++d) {
+                    int nc = cc + d, ic = nc < 0 ? -1 : (nc >= g.n[2] ? 1 : 0);
+                    nc -= ic * g.n[2];
+                    int cell = S.cell_off + g.flat(na, nb, nc);
+                    float2 sx = make_float2(xi.x - ia * S.Lf.x, xi.x - ia * S.Lf.x);
+                    float2 sy = make_float2(xi.y - ib * S.Lf.y, xi.y - ib * S.Lf.y);
+                    float2 sz = make_float2(xi.z - ic * S.Lf.z, xi.z - ic * S.Lf.z);
+                    unsigned code = (unsigned)image_code(a, b, d) << kSlotBits;
+                    int js = start[cell], je = start[cell + 1];
+                    for (int j0 = js; j0 < je; j0 += 32) {
+                        int cntj = min(32, je - j0);
+                        __syncwarp();
+                        float4 q = lane < cntj ? posf[j0 + lane] : make_float4(1e18f, 1e18f, 1e18f, 0.f);
+                        cxs[warp][0][lane] = -q.x;
+                        cxs[warp][1][lane] = -q.y;
+                        cxs[warp][2][lane] = -q.z;
+                        __syncwarp();
+                        unsigned mask = 0;
+                        for (int t = 0; t < cntj; t += 2) {
+                            float2 qx = *reinterpret_cast<const float2*>(&cxs[warp][0][t]);
+                            float2 qy = *reinterpret_cast<const float2*>(&cxs[warp][1][t]);
+                            float2 qz = *reinterpret_cast<const float2*>(&cxs[warp][2][t]);
+                            float2 dx = __fadd2_rn(sx, qx), dy = __fadd2_rn(sy, qy), dz = __fadd2_rn(sz, qz);
+                            float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+                            mask |= (r2.x < S.cut2 ? 1u : 0u) << t;
+                            mask |= (r2.y < S.cut2 ? 2u : 0u) << t;
+                        }
+                        if (cntj < 32) mask &= (1u << cntj) - 1u;
+                        unsigned self = (unsigned)(i - j0);
+                        if (self < 32u) mask &= ~(1u << self);
+                        if (!own) mask = 0;
+                        while (mask) {
+                            int t = __ffs(mask) - 1;
+                            mask &= mask - 1;
+                            append_entry(grp, n, cap, (unsigned)(j0 + t) | code, nbr4, Ntot, i);
+                        }
+                    }
+                }
+            }
+        }
+        if (own) {
+            int m = n < cap ? n : cap;
+            cnt[i] = m;
+            if (m & 3) {
+                for (int k = m & 3; k < 4; ++k) grp[k] = (unsigned)Ntot | (13u << kSlotBits);
+                nbr4[(size_t)(m >> 2) * Ntot + i] = make_uint4(grp[0], grp[1], grp[2], grp[3]);
+            }
+            wmax = max(wmax, n);
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) wmax = max(wmax, __shfl_down_sync(0xffffffffu, wmax, off));
+    if (lane == 0 && wmax > cap) atomicExch(&fl->overflow, 1);
+    if (lc == 0 && lane == 0) atomicAdd((unsigned long long*)&st[sidx].builds, 1ull);
+}
+
+// ---- pair force: per block one system, same loop as force_fp64_kernel ---------
+static __global__ void __launch_bounds__(kThreads, 4)
+b_force_kernel(const int* __restrict__ blk_sys, const int* __restrict__ blk_first, const SysDev* __restrict__ sys,
+               const SysState* st, int Ntot, const double4* __restrict__ pos, Soa s, const uint4* __restrict__ nbr4,
+               const int* __restrict__ cnt, double* __restrict__ partials) {
+    int sidx = blk_sys[blockIdx.x];
+    if (!st[sidx].active) return;
+    const SysDev& S = sys[sidx];
+    const PairParams pp = S.pp;
+    int i = blk_first[blockIdx.x] + threadIdx.x;
+    double acc[4] = {0, 0, 0, 0};
+    if (i < S.atom_off + S.natoms) {
+        const double4 xi = pos[i];
+        bool near = !(xi.x >= pp.near_lo && xi.x < pp.near_hi[0] && xi.y >= pp.near_lo &&
+                      xi.y < pp.near_hi[1] && xi.z >= pp.near_lo && xi.z < pp.near_hi[2]);
+        double fx = 0, fy = 0, fz = 0, pe = 0, w = 0;
+        int ng = (cnt[i] + 3) >> 2;
+        uint4 cur = ng > 0 ? __ldcs(&nbr4[i]) : make_uint4(0, 0, 0, 0);
+        for (int g = 0; g < ng; ++g) {
+            uint4 nxt = g + 1 < ng ? __ldcs(&nbr4[(size_t)(g + 1) * Ntot + i]) : cur;
+            unsigned e[4] = {cur.x, cur.y, cur.z, cur.w};
+            double4 q[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) q[u] = pos[e[u] & kSlotMask];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                double dx, dy, dz, f, V, W;
+                separation<false>(xi, q[u], e[u], near, pp, dx, dy, dz);
+                pair_fp64<KIND_LJ>(pp, norm2(dx, dy, dz), f, V, W);
+                fx = fma(f, dx, fx);
+                fy = fma(f, dy, fy);
+                fz = fma(f, dz, fz);
+                pe += V;
+                w += W;
+            }
+            cur = nxt;
+        }
+        s.at(FX, i) = fx;
+        s.at(FY, i) = fy;
+        s.at(FZ, i) = fz;
+        acc[1] = pe;
+        acc[2] = w;
+        double f3[3] = {fx, fy, fz};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            double v = kick(s.at(VX + k, i), f3[k], pp.dt);
+            s.at(VX + k, i) = v;
+            acc[0] = fma(v, v, acc[0]);
+            double d = s.at(DX + k, i);
+            acc[3] = fma(d, d, acc[3]);
+        }
+    }
+    block_sum<4, kThreads>(acc);
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 4; ++q) partials[(size_t)blockIdx.x * 4 + q] = acc[q];
+}
+
+// One block per system: the single-system finalize over that system's blocks.
+static __global__ void __launch_bounds__(1024)
+b_finalize_kernel(const SysDev* __restrict__ sys, SysState* st, int nsys, const double* __restrict__ partials,
+                  double* __restrict__ ring, int ring_cap, int mode, BatchFlags* fl) {
+    int sidx = blockIdx.x;
+    const SysDev& S = sys[sidx];
+    SysState& T = st[sidx];
+    if (mode == 0 && !T.active) return;
+    double acc[4] = {0, 0, 0, 0};
+    for (int b = threadIdx.x; b < S.nblk; b += blockDim.x)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[q] += partials[(size_t)(S.blk_off + b) * 4 + q];
+    block_sum<4, 1024>(acc);
+    if (threadIdx.x == 0) {
+        if (mode != 2) {
+            T.pe = 0.5 * acc[1];
+            T.vir = 0.5 * acc[2];
+        }
+        double* out = ring + 7 * ((size_t)(mode == 0 ? fl->slot : ring_cap) * nsys + sidx);
+        if (mode == 0) {
+            T.t = T.t + S.pp.dt;
+            T.steps += 1;
+        }
+        double ke = 0.5 * acc[0];
+        if (mode != 1) {
+            out[0] = T.t;
+            out[1] = ke;
+            out[2] = T.pe;
+            out[3] = T.pe + ke;
+            out[4] = T.vir;
+            out[5] = (2. / 3.) * ke / (double)S.natoms;
+            out[6] = acc[3] / (double)S.natoms;
+        }
+        if (!isfinite(ke) || !isfinite(T.pe) || !isfinite(T.vir)) atomicExch(&fl->nonfinite, 1);
+        if (mode == 0) {
+            T.max_disp2 = 0ull;
+            T.need_rebuild = 0;
+            T.rebuild = 0;
+        }
+    }
+}
+
+// Measurement partial sums without a step (for set_temperature / measure).
+static __global__ void __launch_bounds__(kThreads)
+b_measure_kernel(const int* __restrict__ blk_sys, const int* __restrict__ blk_first, const SysDev* __restrict__ sys,
+                 Soa s, double* __restrict__ partials) {
+    int sidx = blk_sys[blockIdx.x];
+    const SysDev& S = sys[sidx];
+    int i = blk_first[blockIdx.x] + threadIdx.x;
+    double acc[4] = {0, 0, 0, 0};
+    if (i < S.atom_off + S.natoms) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            double v = s.at(VX + k, i), d = s.at(DX + k, i);
+            acc[0] = fma(v, v, acc[0]);
+            acc[3] = fma(d, d, acc[3]);
+        }
+    }
+    block_sum<4, kThreads>(acc);
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 4; ++q) partials[(size_t)blockIdx.x * 4 + q] = acc[q];
+}
+
+static __global__ void __launch_bounds__(kThreads)
+b_scale_kernel(int first, int n, Soa s, double factor) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) s.at(VX + k, first + i) = __dmul_rn(s.at(VX + k, first + i), factor);
+}
+
+static __global__ void b_unpack_kernel(int first, int n, const double* __restrict__ in, int stride, int field,
+                                       double4* __restrict__ pos, Soa s, int* __restrict__ ids) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double* p = in + (size_t)i * stride;
+    int k = first + i;
+    if (field < 0) {
+        pos[k] = make_double4(p[0], p[1], p[2], 0.0);
+        ids[k] = i;
+    } else {
+        for (int q = 0; q < 3; ++q) s.at(field + q, k) = p[q];
+    }
+}
+
+static __global__ void b_pack_kernel(int first, int n, double* __restrict__ out, int stride, int field,
+                                     const double4* __restrict__ pos, Soa s, const int* __restrict__ ids) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int slot = first + k;
+    double* p = out + (size_t)ids[slot] * stride;
+    double v[3];
+    if (field < 0) {
+        double4 x = pos[slot];
+        v[0] = x.x; v[1] = x.y; v[2] = x.z;
+    } else {
+        for (int q = 0; q < 3; ++q) v[q] = s.at(field + q, slot);
+    }
+    for (int q = 0; q < 3; ++q) p[q] = v[q];
+    if (stride == 4) p[3] = 0.0;
+}
+
+int hiword_b(double x) {
+    long long b;
+    std::memcpy(&b, &x, 8);
+    return (int)(b >> 32);
+}
+
+}  // namespace
+
+struct lj_batch {
+    int nsys = 0, Ntot = 0, ncell = 0, nblk = 0, cap = 0, device = 0;
+    cudaStream_t stream = nullptr, side = nullptr;
+    std::vector<SysDev> hsys;
+    SysDev* sys = nullptr;
+    SysState* st = nullptr;
+    BatchFlags* fl = nullptr;
+    int *blk_sys = nullptr, *blk_first = nullptr, *sys_of = nullptr, *cell_sys = nullptr;
+    double4 *pos = nullptr, *pos_tmp = nullptr;
+    float4* posf = nullptr;
+    double *soa = nullptr, *soa_tmp = nullptr, *bd = nullptr, *partials = nullptr, *ring = nullptr;
+    double* host_ring = nullptr;
+    int ring_cap = 256;
+    int *ids = nullptr, *ids_tmp = nullptr, *cell_of = nullptr, *rank = nullptr, *order = nullptr;
+    int *count = nullptr, *start = nullptr, *cnt = nullptr;
+    uint4* nbr = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    bool graph_tried = false;
+    long long host_steps = 0;
+    long long launches = 0;
+    char err[512] = {0};
+};
+
+namespace {
+
+#define BK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) {                                                                  \
+            std::snprintf(b->err, sizeof b->err, "%s: %s", #call, cudaGetErrorString(e_));        \
+            return LJ_ERR_CUDA;                                                                   \
+        }                                                                                         \
+    } while (0)
+#define BKL()                                                                                      \
+    do {                                                                                           \
+        ++b->launches;                                                                             \
+        cudaError_t e_ = cudaGetLastError();                                                       \
+        if (e_ != cudaSuccess) {                                                                   \
+            std::snprintf(b->err, sizeof b->err, "launch: %s", cudaGetErrorString(e_));            \
+            return LJ_ERR_CUDA;                                                                    \
+        }                                                                                          \
+    } while (0)
+
+int nb(int n, int t = kThreads) { return (n + t - 1) / t; }
+
+int launch_rebuild_b(lj_batch* b) {
+    Soa s{b->soa, b->Ntot}, st{b->soa_tmp, b->Ntot};
+    b_bin_kernel<<<nb(b->Ntot), kThreads, 0, b->stream>>>(b->sys_of, b->sys, b->st, b->Ntot, b->pos, b->cell_of,
+                                                          b->rank, b->count);
+    BKL();
+    b_scan_kernel<<<b->nsys, 1024, 0, b->stream>>>(b->sys, b->st, b->count, b->start);
+    BKL();
+    b_scatter_kernel<<<nb(b->Ntot), kThreads, 0, b->stream>>>(b->sys_of, b->st, b->Ntot, b->cell_of, b->rank,
+                                                              b->start, b->order);
+    BKL();
+    b_cell_sort_kernel<<<nb(b->ncell, kSortWarps), 32 * kSortWarps, 0, b->stream>>>(b->cell_sys, b->st, b->ncell,
+                                                                                   b->start, b->order);
+    BKL();
+    b_gather_kernel<<<nb(b->Ntot), kThreads, 0, b->stream>>>(b->sys_of, b->st, b->Ntot, b->order, b->pos,
+                                                             b->pos_tmp, s, st, b->ids, b->ids_tmp, b->bd);
+    BKL();
+    b_copy_back_kernel<<<nb(b->Ntot), kThreads, 0, b->stream>>>(b->sys_of, b->st, b->Ntot, b->pos_tmp, b->pos, st, s,
+                                                                b->ids_tmp, b->ids, b->posf);
+    BKL();
+    b_build_list_kernel<<<nb(b->ncell, kBuildWarps), 32 * kBuildWarps, 0, b->stream>>>(
+        b->cell_sys, b->sys, b->st, b->ncell, b->Ntot, b->posf, b->start, b->cap, b->nbr, b->cnt, b->fl);
+    BKL();
+    return LJ_OK;
+}
+
+int launch_step_b(lj_batch* b, cudaGraphConditionalHandle* h) {
+    Soa s{b->soa, b->Ntot};
+    b_kick_drift_kernel<<<b->nblk, kThreads, 0, b->stream>>>(b->blk_sys, b->blk_first, b->sys, b->st, b->Ntot, b->pos,
+                                                             s, b->bd);
+    BKL();
+    b_decide_kernel<<<1, 256, 0, b->stream>>>(b->sys, b->st, b->nsys, b->fl, b->ring_cap,
+                                              h ? *h : cudaGraphConditionalHandle{}, h ? 1 : 0);
+    BKL();
+    return LJ_OK;
+}
+
+int launch_force_b(lj_batch* b) {
+    Soa s{b->soa, b->Ntot};
+    b_force_kernel<<<b->nblk, kThreads, 0, b->stream>>>(b->blk_sys, b->blk_first, b->sys, b->st, b->Ntot, b->pos, s,
+                                                        b->nbr, b->cnt, b->partials);
+    BKL();
+    b_finalize_kernel<<<b->nsys, 1024, 0, b->stream>>>(b->sys, b->st, b->nsys, b->partials, b->ring, b->ring_cap, 0,
+                                                       b->fl);
+    BKL();
+    return LJ_OK;
+}
+
+// One step launched kernel by kernel (the rebuild chain always runs; its kernels skip
+// the systems that do not rebuild).
+int direct_step_b(lj_batch* b) {
+    int rc = launch_step_b(b, nullptr);
+    if (!rc) rc = launch_rebuild_b(b);
+    if (!rc) rc = launch_force_b(b);
+    return rc;
+}
+
+constexpr int kBatchGraphSteps = 8;
+
+int build_graph_b(lj_batch* b) {
+    cudaStream_t main = b->stream;
+    long long l0 = b->launches;
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(main, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return LJ_ERR_CUDA;
+    int rc = LJ_OK;
+    for (int k = 0; k < kBatchGraphSteps && rc == LJ_OK; ++k) {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t g = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        cudaGraphConditionalHandle h;
+        if (cudaStreamGetCaptureInfo(main, &cs, nullptr, &g, &deps, &ndeps) != cudaSuccess ||
+            cudaGraphConditionalHandleCreate(&h, g, 0, 0) != cudaSuccess) {
+            rc = LJ_ERR_CUDA;
+            break;
+        }
+        if ((rc = launch_step_b(b, &h))) break;
+        if (cudaStreamGetCaptureInfo(main, &cs, nullptr, &g, &deps, &ndeps) != cudaSuccess) {
+            rc = LJ_ERR_CUDA;
+            break;
+        }
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        cudaGraphNode_t cnode;
+        if (cudaGraphAddNode(&cnode, g, deps, ndeps, &cp) != cudaSuccess ||
+            cudaStreamUpdateCaptureDependencies(main, &cnode, 1, cudaStreamSetCaptureDependencies) != cudaSuccess ||
+            cudaStreamBeginCaptureToGraph(b->side, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            rc = LJ_ERR_CUDA;
+            break;
+        }
+        b->stream = b->side;
+        rc = launch_rebuild_b(b);
+        b->stream = main;
+        cudaGraph_t body = nullptr;
+        if (cudaStreamEndCapture(b->side, &body) != cudaSuccess && rc == LJ_OK) rc = LJ_ERR_CUDA;
+        if (rc) break;
+        rc = launch_force_b(b);
+    }
+    b->stream = main;
+    e = cudaStreamEndCapture(main, &graph);
+    b->launches = l0;
+    if (rc == LJ_OK && e == cudaSuccess && cudaGraphInstantiate(&b->graph, graph, 0) == cudaSuccess) {
+        b->graph_steps = kBatchGraphSteps;
+    } else {
+        b->graph = nullptr;
+        rc = LJ_ERR_CUDA;
+        cudaGetLastError();
+    }
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+}
+
+int enqueue_b(lj_batch* b, int nsteps) {
+    if (!b->graph_tried) {
+        b->graph_tried = true;
+        build_graph_b(b);
+    }
+    int s = 0;
+    if (b->graph_steps > 0)
+        for (; s + b->graph_steps <= nsteps; s += b->graph_steps) BK(cudaGraphLaunch(b->graph, b->stream));
+    for (; s < nsteps; ++s) {
+        int rc = direct_step_b(b);
+        if (rc) return rc;
+    }
+    b->host_steps += nsteps;
+    return LJ_OK;
+}
+
+int read_flags_b(lj_batch* b) {
+    BatchFlags h;
+    BK(cudaMemcpyAsync(&h, b->fl, sizeof h, cudaMemcpyDeviceToHost, b->stream));
+    BK(cudaStreamSynchronize(b->stream));
+    if (h.overflow) {
+        std::snprintf(b->err, sizeof b->err, "neighbour list capacity exceeded");
+        return LJ_ERR_CAPACITY;
+    }
+    if (h.nonfinite) {
+        std::snprintf(b->err, sizeof b->err, "non-finite energy or virial");
+        return LJ_ERR_NONFINITE;
+    }
+    return LJ_OK;
+}
+
+void free_b(lj_batch* b) {
+    void* ptrs[] = {b->sys, b->st, b->fl, b->blk_sys, b->blk_first, b->sys_of, b->cell_sys, b->pos, b->pos_tmp,
+                    b->posf, b->soa, b->soa_tmp, b->bd, b->partials, b->ring, b->ids, b->ids_tmp, b->cell_of,
+                    b->rank, b->order, b->count, b->start, b->cnt, b->nbr};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (b->host_ring) cudaFreeHost(b->host_ring);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    if (b->side) cudaStreamDestroy(b->side);
+    if (b->stream) cudaStreamDestroy(b->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+int lj_batch_create(const lj_batch_system* systems, int nsys, double cutoff, int device, lj_batch** out) {
+    if (!systems || nsys < 1 || !out || !(cutoff * cutoff > std::cbrt(2.0))) return LJ_ERR_ARG;
+    *out = nullptr;
+    lj_batch* b = new (std::nothrow) lj_batch();
+    if (!b) return LJ_ERR_ARG;
+    b->nsys = nsys;
+    b->device = device;
+    double rc = cutoff;
+    long long Ntot = 0, ncell = 0, nblk = 0;
+    double rho_max = 0, cutmax = 0;
+    b->hsys.resize((size_t)nsys);
+    for (int s = 0; s < nsys; ++s) {
+        const lj_batch_system& q = systems[s];
+        SysDev& S = b->hsys[(size_t)s];
+        std::memset(&S, 0, sizeof S);
+        if (q.particle_count < 1) { delete b; return LJ_ERR_ARG; }
+        double Lmin = std::min(q.box[0], std::min(q.box[1], q.box[2]));
+        if (!(Lmin >= 3 * rc)) { delete b; return LJ_ERR_ARG; }  // needs >= 3 cells of edge rc per axis
+        double skin = list_skin(q.skin, Lmin, rc);
+        S.atom_off = (int)Ntot;
+        S.natoms = q.particle_count;
+        PairParams& pp = S.pp;
+        pp.rc = rc;
+        pp.rc2 = rc * rc;
+        pp.inv_rc2 = 1.0 / pp.rc2;
+        double rcm6 = 1 / (pp.rc2 * pp.rc2 * pp.rc2);
+        pp.alpha = -4.0 * rcm6 * (rcm6 - 1.0);
+        pp.beta = 12.0 * rcm6 * (2.0 * rcm6 - 1.0);
+        pp.dt = q.time_delta;
+        double near = rc * (1.0 + 1e-9);
+        pp.near_lo = near;
+        double Lmax = 0;
+        for (int k = 0; k < 3; ++k) {
+            pp.L[k] = q.box[k];
+            pp.halfL[k] = 0.5 * q.box[k];
+            pp.halfL_hi[k] = hiword_b(0.5 * q.box[k]);
+            pp.near_hi[k] = q.box[k] - near;
+            S.grid.n[k] = std::max(1, (int)std::floor(q.box[k] / (rc + skin)));
+            S.grid.ratio[k] = (double)S.grid.n[k] / q.box[k];
+            Lmax = std::max(Lmax, q.box[k]);
+        }
+        double h = 0.5 * skin;
+        S.thresh2 = h * h * 0.999;
+        S.always = skin == 0.0 ? 1 : 0;
+        double cut = rc + skin + 8.0 * Lmax * std::ldexp(1.0, -24) + 1e-6;
+        S.cut2 = (float)(cut * cut);
+        S.Lf = make_float3((float)q.box[0], (float)q.box[1], (float)q.box[2]);
+        S.cell_off = (int)ncell;
+        S.ncell = S.grid.ncell();
+        S.blk_off = (int)nblk;
+        S.nblk = (q.particle_count + kThreads - 1) / kThreads;
+        Ntot += q.particle_count;
+        ncell += S.ncell;
+        nblk += S.nblk;
+        rho_max = std::max(rho_max, q.particle_count / (q.box[0] * q.box[1] * q.box[2]));
+        cutmax = std::max(cutmax, rc + skin);
+    }
+    if (Ntot >= kMaxAtoms) { delete b; return LJ_ERR_ARG; }
+    b->Ntot = (int)Ntot;
+    b->ncell = (int)ncell;
+    b->nblk = (int)nblk;
+    double expect = 4.0 / 3.0 * M_PI * cutmax * cutmax * cutmax * std::max(rho_max, 1.2);
+    b->cap = ((int)std::ceil(1.5 * expect + 32) + 3) & ~3;
+    BK(cudaSetDevice(device));
+    BK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    BK(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking));
+    int N = b->Ntot;
+    std::vector<int> blk_sys((size_t)nblk), blk_first((size_t)nblk), sys_of((size_t)N), cell_sys((size_t)ncell);
+    for (int s = 0; s < nsys; ++s) {
+        const SysDev& S = b->hsys[(size_t)s];
+        for (int j = 0; j < S.nblk; ++j) {
+            blk_sys[(size_t)(S.blk_off + j)] = s;
+            blk_first[(size_t)(S.blk_off + j)] = S.atom_off + j * kThreads;
+        }
+        for (int i = 0; i < S.natoms; ++i) sys_of[(size_t)(S.atom_off + i)] = s;
+        for (int c = 0; c < S.ncell; ++c) cell_sys[(size_t)(S.cell_off + c)] = s;
+    }
+    BK(cudaMalloc(&b->sys, sizeof(SysDev) * nsys));
+    BK(cudaMalloc(&b->st, sizeof(SysState) * nsys));
+    BK(cudaMalloc(&b->fl, sizeof(BatchFlags)));
+    BK(cudaMalloc(&b->blk_sys, sizeof(int) * nblk));
+    BK(cudaMalloc(&b->blk_first, sizeof(int) * nblk));
+    BK(cudaMalloc(&b->sys_of, sizeof(int) * N));
+    BK(cudaMalloc(&b->cell_sys, sizeof(int) * ncell));
+    BK(cudaMalloc(&b->pos, sizeof(double4) * (N + 1)));
+    BK(cudaMalloc(&b->pos_tmp, sizeof(double4) * N));
+    BK(cudaMalloc(&b->posf, sizeof(float4) * (N + 1)));
+    BK(cudaMalloc(&b->soa, sizeof(double) * SOA_FIELDS * N));
+    BK(cudaMalloc(&b->soa_tmp, sizeof(double) * SOA_FIELDS * N));
+    BK(cudaMalloc(&b->bd, sizeof(double) * 3 * N));
+    BK(cudaMalloc(&b->partials, sizeof(double) * 4 * nblk));
+    BK(cudaMalloc(&b->ring, sizeof(double) * 7 * (size_t)(b->ring_cap + 1) * nsys));
+    BK(cudaMallocHost(&b->host_ring, sizeof(double) * 7 * (size_t)(b->ring_cap + 1) * nsys));
+    BK(cudaMalloc(&b->ids, sizeof(int) * N));
+    BK(cudaMalloc(&b->ids_tmp, sizeof(int) * N));
+    BK(cudaMalloc(&b->cell_of, sizeof(int) * N));
+    BK(cudaMalloc(&b->rank, sizeof(int) * N));
+    BK(cudaMalloc(&b->order, sizeof(int) * N));
+    BK(cudaMalloc(&b->count, sizeof(int) * ncell));
+    BK(cudaMalloc(&b->start, sizeof(int) * (ncell + 1)));
+    BK(cudaMalloc(&b->cnt, sizeof(int) * N));
+    BK(cudaMalloc(&b->nbr, sizeof(uint4) * (size_t)(b->cap / 4) * N));
+    BK(cudaMemcpy(b->sys, b->hsys.data(), sizeof(SysDev) * nsys, cudaMemcpyHostToDevice));
+    std::vector<SysState> st0((size_t)nsys);
+    for (auto& q : st0) {
+        std::memset(&q, 0, sizeof q);
+        q.active = 1;
+        q.need_rebuild = 1;
+    }
+    BK(cudaMemcpy(b->st, st0.data(), sizeof(SysState) * nsys, cudaMemcpyHostToDevice));
+    BK(cudaMemset(b->fl, 0, sizeof(BatchFlags)));
+    BK(cudaMemcpy(b->blk_sys, blk_sys.data(), sizeof(int) * nblk, cudaMemcpyHostToDevice));
+    BK(cudaMemcpy(b->blk_first, blk_first.data(), sizeof(int) * nblk, cudaMemcpyHostToDevice));
+    BK(cudaMemcpy(b->sys_of, sys_of.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+    BK(cudaMemcpy(b->cell_sys, cell_sys.data(), sizeof(int) * ncell, cudaMemcpyHostToDevice));
+    BK(cudaMemset(b->pos, 0, sizeof(double4) * N));
+    BK(cudaMemset(b->soa, 0, sizeof(double) * SOA_FIELDS * N));
+    BK(cudaMemset(b->bd, 0, sizeof(double) * 3 * N));
+    BK(cudaMemset(b->count, 0, sizeof(int) * ncell));
+    BK(cudaMemset(b->cnt, 0, sizeof(int) * N));
+    const double4 ghost = make_double4(1e18, 1e18, 1e18, 0.0);
+    const float4 ghostf = make_float4(1e18f, 1e18f, 1e18f, 0.f);
+    BK(cudaMemcpy(b->pos + N, &ghost, sizeof ghost, cudaMemcpyHostToDevice));
+    BK(cudaMemcpy(b->posf + N, &ghostf, sizeof ghostf, cudaMemcpyHostToDevice));
+    std::vector<int> ident((size_t)N);
+    for (int s = 0; s < nsys; ++s)
+        for (int i = 0; i < b->hsys[(size_t)s].natoms; ++i) ident[(size_t)(b->hsys[(size_t)s].atom_off + i)] = i;
+    BK(cudaMemcpy(b->ids, ident.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+    int sentinel = N;
+    BK(cudaMemcpy(b->start + ncell, &sentinel, sizeof(int), cudaMemcpyHostToDevice));
+    *out = b;
+    return LJ_OK;
+}
+
+int lj_batch_destroy(lj_batch* b) {
+    if (!b) return LJ_ERR_ARG;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    free_b(b);
+    delete b;
+    return LJ_OK;
+}
+
+const char* lj_batch_last_error(const lj_batch* b) { return b ? b->err : "null batch"; }
+
+int lj_batch_upload_system(lj_batch* b, int sys, const double* x, const double* v, int stride) {
+    if (!b || sys < 0 || sys >= b->nsys || !x || (stride != 3 && stride != 4)) return LJ_ERR_ARG;
+    BK(cudaSetDevice(b->device));
+    const SysDev& S = b->hsys[(size_t)sys];
+    int n = S.natoms;
+    double* stage = reinterpret_cast<double*>(b->pos_tmp) + 4 * (size_t)S.atom_off;  // this system's room
+    Soa s{b->soa, b->Ntot};
+    const double* src[2] = {x, v};
+    int field[2] = {-1, VX};
+    for (int q = 0; q < 2; ++q) {
+        if (!src[q]) {
+            BK(cudaMemsetAsync(b->soa + (size_t)VX * b->Ntot + S.atom_off, 0, sizeof(double) * n, b->stream));
+            BK(cudaMemsetAsync(b->soa + (size_t)VY * b->Ntot + S.atom_off, 0, sizeof(double) * n, b->stream));
+            BK(cudaMemsetAsync(b->soa + (size_t)VZ * b->Ntot + S.atom_off, 0, sizeof(double) * n, b->stream));
+            continue;
+        }
+        BK(cudaMemcpyAsync(stage, src[q], sizeof(double) * stride * n, cudaMemcpyHostToDevice, b->stream));
+        b_unpack_kernel<<<nb(n), kThreads, 0, b->stream>>>(S.atom_off, n, stage, stride, field[q], b->pos, s, b->ids);
+        BKL();
+    }
+    for (int f : {DX, DY, DZ, FX, FY, FZ})
+        BK(cudaMemsetAsync(b->soa + (size_t)f * b->Ntot + S.atom_off, 0, sizeof(double) * n, b->stream));
+    SysState q;
+    std::memset(&q, 0, sizeof q);
+    q.active = 1;
+    q.need_rebuild = 1;
+    BK(cudaMemcpyAsync(b->st + sys, &q, sizeof q, cudaMemcpyHostToDevice, b->stream));
+    BK(cudaStreamSynchronize(b->stream));
+    return LJ_OK;
+}
+
+int lj_batch_download_system(lj_batch* b, int sys, double* x, double* v, double* F, int stride) {
+    if (!b || sys < 0 || sys >= b->nsys || (stride != 3 && stride != 4)) return LJ_ERR_ARG;
+    BK(cudaSetDevice(b->device));
+    const SysDev& S = b->hsys[(size_t)sys];
+    int n = S.natoms;
+    double* stage = reinterpret_cast<double*>(b->pos_tmp) + 4 * (size_t)S.atom_off;
+    Soa s{b->soa, b->Ntot};
+    double* dst[3] = {x, v, F};
+    int field[3] = {-1, VX, FX};
+    for (int q = 0; q < 3; ++q) {
+        if (!dst[q]) continue;
+        b_pack_kernel<<<nb(n), kThreads, 0, b->stream>>>(S.atom_off, n, stage, stride, field[q], b->pos, s, b->ids);
+        BKL();
+        BK(cudaMemcpyAsync(dst[q], stage, sizeof(double) * stride * n, cudaMemcpyDeviceToHost, b->stream));
+    }
+    BK(cudaStreamSynchronize(b->stream));
+    return LJ_OK;
+}
+
+int lj_batch_set_active(lj_batch* b, int sys, int active) {
+    if (!b || sys < 0 || sys >= b->nsys) return LJ_ERR_ARG;
+    BK(cudaSetDevice(b->device));
+    int a = active ? 1 : 0;
+    BK(cudaMemcpyAsync(&b->st[sys].active, &a, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    BK(cudaStreamSynchronize(b->stream));
+    return LJ_OK;
+}
+
+// nsteps steps of every active system; out (may be NULL) receives nsteps x nsys
+// records (step-major; inactive systems' records are left as they were).
+int lj_batch_step(lj_batch* b, int nsteps, lj_thermo* out) {
+    if (!b || nsteps < 0) return LJ_ERR_ARG;
+    BK(cudaSetDevice(b->device));
+    int done = 0;
+    size_t per = 7 * (size_t)b->nsys;
+    while (done < nsteps) {
+        int chunk = std::min(nsteps - done, b->ring_cap);
+        long long first = b->host_steps;
+        int rc = enqueue_b(b, chunk);
+        if (rc) return rc;
+        if (out) {
+            int s0 = (int)(first % b->ring_cap);
+            int n1 = std::min(chunk, b->ring_cap - s0);
+            BK(cudaMemcpyAsync(b->host_ring, b->ring + per * s0, sizeof(double) * per * n1, cudaMemcpyDeviceToHost,
+                               b->stream));
+            if (n1 < chunk)
+                BK(cudaMemcpyAsync(b->host_ring + per * n1, b->ring, sizeof(double) * per * (chunk - n1),
+                                   cudaMemcpyDeviceToHost, b->stream));
+        }
+        if ((rc = read_flags_b(b))) return rc;
+        if (out) std::memcpy(out + (size_t)done * b->nsys, b->host_ring, sizeof(double) * per * chunk);
+        done += chunk;
+    }
+    return LJ_OK;
+}
+
+// Instantaneous measurement of every system: out receives nsys records.
+int lj_batch_measure(lj_batch* b, lj_thermo* out) {
+    if (!b || !out) return LJ_ERR_ARG;
+    BK(cudaSetDevice(b->device));
+    Soa s{b->soa, b->Ntot};
+    b_measure_kernel<<<b->nblk, kThreads, 0, b->stream>>>(b->blk_sys, b->blk_first, b->sys, s, b->partials);
+    BKL();
+    b_finalize_kernel<<<b->nsys, 1024, 0, b->stream>>>(b->sys, b->st, b->nsys, b->partials, b->ring, b->ring_cap, 2,
+                                                       b->fl);
+    BKL();
+    size_t per = 7 * (size_t)b->nsys;
+    BK(cudaMemcpyAsync(b->host_ring, b->ring + per * b->ring_cap, sizeof(double) * per, cudaMemcpyDeviceToHost,
+                       b->stream));
+    BK(cudaStreamSynchronize(b->stream));
+    std::memcpy(out, b->host_ring, sizeof(double) * per);
+    return LJ_OK;
+}
+
+// physics::set_temperature for one system.
+int lj_batch_set_temperature(lj_batch* b, int sys, double target, double* measured) {
+    if (!b || sys < 0 || sys >= b->nsys || !(target >= 0)) return LJ_ERR_ARG;
+    std::vector<lj_thermo> m((size_t)b->nsys);
+    int rc = lj_batch_measure(b, m.data());
+    if (rc) return rc;
+    double T = m[(size_t)sys].temperature;
+    if (!(T > 0)) return LJ_ERR_ARG;
+    if (measured) *measured = T;
+    const SysDev& S = b->hsys[(size_t)sys];
+    Soa s{b->soa, b->Ntot};
+    b_scale_kernel<<<nb(S.natoms), kThreads, 0, b->stream>>>(S.atom_off, S.natoms, s, std::sqrt(target / T));
+    BKL();
+    BK(cudaStreamSynchronize(b->stream));
+    return LJ_OK;
+}
+
+int lj_batch_info(const lj_batch* b, int* total_atoms, long long* builds_per_system, long long* kernel_launches) {
+    if (!b) return LJ_ERR_ARG;
+    if (total_atoms) *total_atoms = b->Ntot;
+    if (builds_per_system) {
+        std::vector<SysState> st((size_t)b->nsys);
+        if (cudaMemcpy(st.data(), b->st, sizeof(SysState) * b->nsys, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return LJ_ERR_CUDA;
+        for (int s = 0; s < b->nsys; ++s) builds_per_system[s] = st[(size_t)s].builds;
+    }
+    if (kernel_launches) *kernel_launches = b->launches;
+    return LJ_OK;
+}
+
+}  // extern "C"

@@ -145,6 +145,20 @@ Gate gate_of(lj_ctx* c) {
 
 Soa soa_of(double* p, int N) { return Soa{p, N}; }
 
+}  // namespace
+
+// Verlet skin for a box: the requested skin (default 0.3), shrunk so the list
+// grid keeps >= 3 cells of edge >= rc + skin per axis (the minimum-image form);
+// 0 (a rebuild every step) when that leaves less than 0.05.
+double list_skin(double requested, double Lmin, double rc) {
+    double skin = requested < 0 ? 0.3 : requested;
+    double fit = Lmin / 3.0 - rc - 1e-9 * Lmin;
+    if (skin > fit) skin = fit;
+    return skin >= 0.05 ? skin : 0.0;
+}
+
+namespace {
+
 // Counting sort of atoms into grid g (histogram, scan, scatter); rank/cell_of per slot.
 template <bool GATED>
 int launch_binning(lj_ctx* ctx, const Grid& g, int* count, int* start, int* tiles, Gate gate) {
@@ -489,9 +503,8 @@ int lj_gpu_create(const lj_params* params, lj_ctx** out) {
 
     // neighbour-list grid: cells of at least rc + skin, and >= 3 per axis for
     // the minimum-image form; otherwise zero skin and a rebuild every step.
-    double skin = p.skin < 0 ? 0.3 : p.skin;
     double Lmin = std::min(p.box[0], std::min(p.box[1], p.box[2]));
-    if (p.force_kind == LJ_FORCE_NONE || std::floor(Lmin / (rc + skin)) < 3) skin = 0.0;
+    double skin = p.force_kind == LJ_FORCE_NONE ? 0.0 : list_skin(p.skin, Lmin, rc);
     ctx->skin = skin;
     ctx->ref_grid = make_grid(p.box, rc);
     ctx->list_grid = make_grid(p.box, rc + skin);

@@ -594,8 +594,10 @@ finalize_kernel(const double* __restrict__ partials, int nblocks, int N, double 
         } else if (!isfinite(sc->pe) || !isfinite(sc->vir)) {
             sc->nonfinite = 1;
         }
-        sc->max_disp2 = 0ull;
-        sc->need_rebuild = 0;
+        if (mode != 2) {  // a measurement changes nothing that a rebuild depends on
+            sc->max_disp2 = 0ull;
+            sc->need_rebuild = 0;
+        }
     }
 }
 

@@ -205,6 +205,135 @@ int lj_pair_along_z(double cutoff, double r, double* out) {
     return LJ_OK;
 }
 
+
+// The control protocol of one simulation, fed one ThermodynamicMeasurement per
+// step.  next_decision() is the first step at which the current phase can act;
+// feed() replays a step's record and reports what the controller asks of the
+// engine (a velocity rescale) and whether the run has finished.
+struct Controller {
+    const lj_sim_config* cfg;
+    Sinks out;
+    int N;
+    int time_step = 0;
+    int phase = 0;  // 0 equilibration, 1 observation, 2 finished
+    int start = 0, last_check = 0, last_adjust = 0, last_obs = 0, count = 0;
+    int outcome = 0, nobs = 0;
+    Window Tw, Ew, Ww, tw, mw;
+    const char* names[2];
+
+    explicit Controller(const lj_sim_config* c)
+        : cfg(c), N(c->particle_count), Tw(c->eq_sample_size), Ew(c->ob_sample_size), Ww(c->ob_sample_size),
+          tw(c->ob_sample_size), mw(c->ob_sample_size) {
+        names[0] = c->eq_name ? c->eq_name : "Equilibration Phase";
+        names[1] = c->ob_name ? c->ob_name : "Observation Phase";
+    }
+
+    int open(int echo) {
+        out.echo = echo;
+        out.events = std::fopen(cfg->event_log, "w");
+        out.thermo = std::fopen(cfg->thermodynamic_log, "w");
+        out.obs = std::fopen(cfg->observation_log, "w");
+        out.snap = std::fopen(cfg->snapshot_log, "w");
+        if (!out.events || !out.thermo || !out.obs || !out.snap) return LJ_ERR_ARG;
+        std::fputs("TimeStep,Time,KineticEnergy,PotentialEnergy,TotalEnergy,Virial,Temperature,"
+                   "MeanSquareDisplacement\n", out.thermo);
+        std::fputs("TimeStep,Temperature,Density,TotalEnergy,Pressure,SpecificHeat,DiffusionCoefficient\n", out.obs);
+        std::fputs("TimeStep,ParticleID,Position,Position,Position,Velocity,Velocity,Velocity,Force,Force,Force\n",
+                   out.snap);
+        std::fputs("TimeStep,ParticleID,X,Y,Z,X,Y,Z,X,Y,Z\n", out.snap);
+        begin_phase();
+        return LJ_OK;
+    }
+
+    void begin_phase() {
+        out.event(time_step, std::string("Phase started: ") + names[phase]);
+        start = last_check = last_adjust = last_obs = time_step;
+        count = 0;
+        Tw = Window(phase == 0 ? cfg->eq_sample_size : cfg->ob_sample_size);
+        Ew = Window(cfg->ob_sample_size);
+        Ww = Window(cfg->ob_sample_size);
+        tw = Window(cfg->ob_sample_size);
+        mw = Window(cfg->ob_sample_size);
+    }
+
+    bool finished() const { return phase == 2; }
+
+    int next_decision() const {
+        if (phase == 0)
+            return std::min({last_check + cfg->eq_adjustment_interval, last_adjust + cfg->eq_steady_state_time,
+                             start + cfg->eq_timeout});
+        return last_obs + cfg->ob_observation_interval;
+    }
+
+    // One step's record.  Returns true when the engine must rescale velocities
+    // to cfg->temperature before the next step.
+    bool feed(const lj_thermo& r) {
+        bool rescale = false;
+        out.thermo_row(time_step, r);  // logged before the increment (simulation_controller.cpp:65-67)
+        time_step += 1;
+        if (phase == 0) {
+            Tw.push(r.temperature);
+            if (time_step - last_check >= cfg->eq_adjustment_interval) {
+                last_check = time_step;
+                double Tm = Tw.mean();
+                if (relative_error(Tm, cfg->temperature) >= cfg->eq_tolerance) {
+                    last_adjust = time_step;
+                    rescale = true;
+                    out.event(time_step, "Temperature measured at: " + fmt_g4(Tm) +
+                                             ", adjusted to: " + fmt_g4(cfg->temperature));
+                }
+            }
+            if (time_step - last_adjust >= cfg->eq_steady_state_time) {
+                out.event(time_step, std::string("Phase complete: ") + names[0]);
+                phase = 1;
+                begin_phase();
+            } else if (time_step - start >= cfg->eq_timeout) {
+                out.event(time_step, "Simulation aborted: Could not equilibrate");
+                phase = 2;
+                outcome = 1;
+            }
+        } else if (phase == 1) {
+            Tw.push(r.temperature);
+            Ew.push(r.total_energy);
+            Ww.push(r.virial);
+            tw.push(r.time);
+            mw.push(r.mean_square_displacement);
+            if (time_step - last_obs >= cfg->ob_observation_interval) {
+                last_obs = time_step;
+                Observation o = analyze(Tw, Ew, Ww, tw, mw, N, cfg->density);
+                if (relative_error(o.temperature, cfg->temperature) >= cfg->ob_tolerance) {
+                    out.event(time_step, "Simulation aborted: Temperature drifted outside acceptable range");
+                    phase = 2;
+                    outcome = 2;
+                    return false;
+                }
+                ++count;
+                ++nobs;
+                out.obs_row(time_step, o);
+                out.event(time_step, "Observation recorded");
+            }
+            if (count >= cfg->ob_observation_count) {
+                out.event(time_step, std::string("Phase complete: ") + names[1]);
+                phase = 2;
+            }
+        }
+        return rescale;
+    }
+
+    // snapshot of the final (or aborted) state (simulation_controller.cpp:100-108, :128-134)
+    void snapshot(const double* x, const double* v, const double* F) {
+        std::string step = std::to_string(time_step) + ",";
+        std::string line;
+        for (int i = 0; i < N; ++i) {
+            line = step + std::to_string(i);
+            for (const double* a : {x, v, F})
+                for (int k = 0; k < 3; ++k) line += "," + fmt_double(a[4 * (size_t)i + k]);
+            line += "\n";
+            std::fputs(line.c_str(), out.snap);
+        }
+    }
+};
+
 int lj_sim_run(const lj_sim_config* cfg, int echo, lj_sim_result* result) {
     if (!cfg || cfg->particle_count < 1 || !cfg->event_log || !cfg->thermodynamic_log || !cfg->observation_log ||
         !cfg->snapshot_log)
@@ -225,130 +354,109 @@ int lj_sim_run(const lj_sim_config* cfg, int echo, lj_sim_result* result) {
     p.device = cfg->device;
     lj_ctx* ctx = nullptr;
     if ((rc = lj_gpu_create(&p, &ctx))) return rc;
-    if ((rc = lj_gpu_upload_state(ctx, x.data(), v.data(), nullptr, nullptr, 4, 0.0, 0.0, 0.0))) {
+    Controller ctl(cfg);
+    if ((rc = lj_gpu_upload_state(ctx, x.data(), v.data(), nullptr, nullptr, 4, 0.0, 0.0, 0.0)) ||
+        (rc = ctl.open(echo))) {
+        ctl.out.close();
         lj_gpu_destroy(ctx);
         return rc;
     }
-
-    Sinks out;
-    out.echo = echo;
-    out.events = std::fopen(cfg->event_log, "w");
-    out.thermo = std::fopen(cfg->thermodynamic_log, "w");
-    out.obs = std::fopen(cfg->observation_log, "w");
-    out.snap = std::fopen(cfg->snapshot_log, "w");
-    if (!out.events || !out.thermo || !out.obs || !out.snap) {
-        out.close();
-        lj_gpu_destroy(ctx);
-        return LJ_ERR_ARG;
-    }
-    std::fputs("TimeStep,Time,KineticEnergy,PotentialEnergy,TotalEnergy,Virial,Temperature,MeanSquareDisplacement\n",
-               out.thermo);
-    std::fputs("TimeStep,Temperature,Density,TotalEnergy,Pressure,SpecificHeat,DiffusionCoefficient\n", out.obs);
-    std::fputs("TimeStep,ParticleID,Position,Position,Position,Velocity,Velocity,Velocity,Force,Force,Force\n",
-               out.snap);
-    std::fputs("TimeStep,ParticleID,X,Y,Z,X,Y,Z,X,Y,Z\n", out.snap);
-
-    int time_step = 0;
-    int outcome = 0, nobs = 0;
-    bool aborted = false;
     std::vector<lj_thermo> recs;
-    const char* names[2] = {cfg->eq_name ? cfg->eq_name : "Equilibration Phase",
-                            cfg->ob_name ? cfg->ob_name : "Observation Phase"};
-    for (int phase = 0; phase < 2 && !aborted && rc == LJ_OK; ++phase) {
-        bool eq = phase == 0;
-        out.event(time_step, std::string("Phase started: ") + names[phase]);
-        int start = time_step, last_check = time_step, last_adjust = time_step, last_obs = time_step;
-        int count = 0;
-        Window Tw(eq ? cfg->eq_sample_size : cfg->ob_sample_size);
-        Window Ew(cfg->ob_sample_size), Ww(cfg->ob_sample_size), tw(cfg->ob_sample_size), mw(cfg->ob_sample_size);
-        bool done = false;
-        while (!done) {
-            // steps until the next step at which this phase can act
-            int next = eq ? std::min({last_check + cfg->eq_adjustment_interval, last_adjust + cfg->eq_steady_state_time,
-                                      start + cfg->eq_timeout})
-                          : last_obs + cfg->ob_observation_interval;
-            int K = std::max(1, next - time_step);
-            recs.resize((size_t)K);
-            if ((rc = lj_gpu_step(ctx, K, recs.data()))) break;
-            for (int k = 0; k < K && !done; ++k) {
-                const lj_thermo& r = recs[(size_t)k];
-                out.thermo_row(time_step, r);  // logged before the increment (simulation_controller.cpp:65-67)
-                time_step += 1;
-                if (eq) {
-                    Tw.push(r.temperature);
-                    if (time_step - last_check >= cfg->eq_adjustment_interval) {
-                        last_check = time_step;
-                        double Tm = Tw.mean();
-                        if (relative_error(Tm, cfg->temperature) >= cfg->eq_tolerance) {
-                            last_adjust = time_step;
-                            if ((rc = lj_gpu_set_temperature(ctx, cfg->temperature, nullptr))) {
-                                done = true;
-                                break;
-                            }
-                            out.event(time_step, "Temperature measured at: " + fmt_g4(Tm) +
-                                                     ", adjusted to: " + fmt_g4(cfg->temperature));
-                        }
-                    }
-                    if (time_step - last_adjust >= cfg->eq_steady_state_time) {
-                        out.event(time_step, std::string("Phase complete: ") + names[phase]);
-                        done = true;
-                    } else if (time_step - start >= cfg->eq_timeout) {
-                        out.event(time_step, "Simulation aborted: Could not equilibrate");
-                        done = aborted = true;
-                        outcome = 1;
-                    }
-                } else {
-                    Tw.push(r.temperature);
-                    Ew.push(r.total_energy);
-                    Ww.push(r.virial);
-                    tw.push(r.time);
-                    mw.push(r.mean_square_displacement);
-                    if (time_step - last_obs >= cfg->ob_observation_interval) {
-                        last_obs = time_step;
-                        Observation o = analyze(Tw, Ew, Ww, tw, mw, N, cfg->density);
-                        if (relative_error(o.temperature, cfg->temperature) >= cfg->ob_tolerance) {
-                            out.event(time_step, "Simulation aborted: Temperature drifted outside acceptable range");
-                            done = aborted = true;
-                            outcome = 2;
-                            continue;
-                        }
-                        ++count;
-                        ++nobs;
-                        out.obs_row(time_step, o);
-                        out.event(time_step, "Observation recorded");
-                    }
-                    if (count >= cfg->ob_observation_count) {
-                        out.event(time_step, std::string("Phase complete: ") + names[phase]);
-                        done = true;
-                    }
-                }
-            }
-        }
+    while (!ctl.finished() && rc == LJ_OK) {
+        int K = std::max(1, ctl.next_decision() - ctl.time_step);
+        recs.resize((size_t)K);
+        if ((rc = lj_gpu_step(ctx, K, recs.data()))) break;
+        for (int k = 0; k < K && !ctl.finished(); ++k)
+            if (ctl.feed(recs[(size_t)k]) && (rc = lj_gpu_set_temperature(ctx, cfg->temperature, nullptr))) break;
     }
-    // snapshot of the final (or aborted) state (simulation_controller.cpp:100-108, :128-134)
     if (rc == LJ_OK) {
         std::vector<double> F(4 * (size_t)N);
-        if ((rc = lj_gpu_download_state(ctx, x.data(), v.data(), nullptr, F.data(), 4, nullptr, nullptr, nullptr)) ==
-            LJ_OK) {
-            std::string step = std::to_string(time_step) + ",";
-            std::string line;
-            for (int i = 0; i < N; ++i) {
-                line = step + std::to_string(i);
-                for (const double* a : {x.data(), v.data(), F.data()})
-                    for (int k = 0; k < 3; ++k) line += "," + fmt_double(a[4 * (size_t)i + k]);
-                line += "\n";
-                std::fputs(line.c_str(), out.snap);
+        rc = lj_gpu_download_state(ctx, x.data(), v.data(), nullptr, F.data(), 4, nullptr, nullptr, nullptr);
+        if (rc == LJ_OK) ctl.snapshot(x.data(), v.data(), F.data());
+    }
+    ctl.out.close();
+    lj_gpu_destroy(ctx);
+    if (result) {
+        result->time_steps = ctl.time_step;
+        result->outcome = ctl.outcome;
+        result->observations = ctl.nobs;
+        result->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return rc;
+}
+
+// A whole sweep on one batched engine: every configuration's control protocol
+// runs on the host as in lj_sim_run, all systems step together, and each chunk
+// ends at the earliest step at which any running simulation can act.  The
+// configurations must share cutoff and time step.
+int lj_sim_run_batch(const lj_sim_config* cfgs, int n, int echo, lj_sim_result* results) {
+    if (!cfgs || n < 1) return LJ_ERR_ARG;
+    auto t0 = std::chrono::steady_clock::now();
+    std::vector<lj_batch_system> systems((size_t)n);
+    std::vector<std::vector<double>> xs((size_t)n), vs((size_t)n);
+    for (int s = 0; s < n; ++s) {
+        const lj_sim_config& c = cfgs[s];
+        if (c.particle_count < 1 || c.cutoff_distance != cfgs[0].cutoff_distance ||
+            c.time_delta != cfgs[0].time_delta)
+            return LJ_ERR_ARG;
+        xs[(size_t)s].resize(4 * (size_t)c.particle_count);
+        vs[(size_t)s].resize(4 * (size_t)c.particle_count);
+        double side = 0;
+        int rc = lj_initial_condition(c.particle_count, c.temperature, c.density, c.random_seed,
+                                      xs[(size_t)s].data(), vs[(size_t)s].data(), &side);
+        if (rc) return rc;
+        systems[(size_t)s].particle_count = c.particle_count;
+        systems[(size_t)s].box[0] = systems[(size_t)s].box[1] = systems[(size_t)s].box[2] = side;
+        systems[(size_t)s].time_delta = c.time_delta;
+        systems[(size_t)s].skin = -1.0;
+    }
+    lj_batch* b = nullptr;
+    int rc = lj_batch_create(systems.data(), n, cfgs[0].cutoff_distance, cfgs[0].device, &b);
+    if (rc) return rc;
+    std::vector<Controller> ctl;
+    ctl.reserve((size_t)n);
+    for (int s = 0; s < n; ++s) ctl.emplace_back(&cfgs[s]);
+    for (int s = 0; s < n && rc == LJ_OK; ++s) {
+        rc = lj_batch_upload_system(b, s, xs[(size_t)s].data(), vs[(size_t)s].data(), 4);
+        if (rc == LJ_OK) rc = ctl[(size_t)s].open(echo);
+    }
+    std::vector<lj_thermo> recs;
+    int running = n;
+    while (running > 0 && rc == LJ_OK) {
+        int K = 1 << 30;
+        for (auto& c : ctl)
+            if (!c.finished()) K = std::min(K, c.next_decision() - c.time_step);
+        K = std::max(1, K);
+        recs.resize((size_t)K * n);
+        if ((rc = lj_batch_step(b, K, recs.data()))) break;
+        for (int s = 0; s < n && rc == LJ_OK; ++s) {
+            Controller& c = ctl[(size_t)s];
+            if (c.finished()) continue;
+            bool rescale = false;
+            for (int k = 0; k < K && !c.finished(); ++k) rescale = c.feed(recs[(size_t)k * n + s]) || rescale;
+            // a rescale precedes an abort on the same step, as in the reference's command queue
+            if (rescale) rc = lj_batch_set_temperature(b, s, cfgs[s].temperature, nullptr);
+            if (rc == LJ_OK && c.finished()) {
+                const int N = cfgs[s].particle_count;
+                std::vector<double> F(4 * (size_t)N);
+                rc = lj_batch_download_system(b, s, xs[(size_t)s].data(), vs[(size_t)s].data(), F.data(), 4);
+                if (rc == LJ_OK) c.snapshot(xs[(size_t)s].data(), vs[(size_t)s].data(), F.data());
+                if (rc == LJ_OK) rc = lj_batch_set_active(b, s, 0);
+                --running;
             }
         }
     }
-    out.close();
-    lj_gpu_destroy(ctx);
-    if (result) {
-        result->time_steps = time_step;
-        result->outcome = outcome;
-        result->observations = nobs;
-        result->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    for (int s = 0; s < n; ++s) {
+        ctl[(size_t)s].out.close();
+        if (results) {
+            results[s].time_steps = ctl[(size_t)s].time_step;
+            results[s].outcome = ctl[(size_t)s].outcome;
+            results[s].observations = ctl[(size_t)s].nobs;
+            results[s].seconds = secs;
+        }
     }
+    lj_batch_destroy(b);
     return rc;
 }
 

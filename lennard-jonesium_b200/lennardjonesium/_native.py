@@ -79,6 +79,11 @@ class SimResult(ctypes.Structure):
                 ("observations", ctypes.c_int), ("seconds", ctypes.c_double)]
 
 
+class BatchSystem(ctypes.Structure):
+    _fields_ = [("particle_count", ctypes.c_int), ("box", ctypes.c_double * 3),
+                ("time_delta", ctypes.c_double), ("skin", ctypes.c_double)]
+
+
 class LJError(RuntimeError):
     """A C-ABI call returned a non-zero status."""
 
@@ -116,8 +121,19 @@ SIGNATURES = {
     "lj_gpu_fma_peaks": (ctypes.c_int, [ctypes.c_int, P, P]),
     "lj_gpu_rdf_noalloc": (ctypes.c_int, [P, ctypes.c_int, P, ctypes.c_int, ctypes.c_double, P, P]),
     "lj_sim_run": (ctypes.c_int, [P, ctypes.c_int, P]),
+    "lj_sim_run_batch": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, P]),
     "lj_format_double": (ctypes.c_int, [ctypes.c_double, ctypes.c_char_p, ctypes.c_int]),
     "lj_pair_along_z": (ctypes.c_int, [ctypes.c_double, ctypes.c_double, P]),
+    "lj_batch_create": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double, ctypes.c_int, P]),
+    "lj_batch_destroy": (ctypes.c_int, [P]),
+    "lj_batch_last_error": (ctypes.c_char_p, [P]),
+    "lj_batch_upload_system": (ctypes.c_int, [P, ctypes.c_int, P, P, ctypes.c_int]),
+    "lj_batch_download_system": (ctypes.c_int, [P, ctypes.c_int, P, P, P, ctypes.c_int]),
+    "lj_batch_set_active": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int]),
+    "lj_batch_step": (ctypes.c_int, [P, ctypes.c_int, P]),
+    "lj_batch_measure": (ctypes.c_int, [P, P]),
+    "lj_batch_set_temperature": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double, P]),
+    "lj_batch_info": (ctypes.c_int, [P, P, P, P]),
     "lj_initial_condition": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                             ctypes.c_uint, P, P, P]),
 }

@@ -33,6 +33,14 @@ def _as4(a, N):
     return out
 
 
+def lattice_side(N, density):
+    """Edge of the cubic box engine::InitialCondition builds (tools/cubic_lattice.cpp:43-58)."""
+    import math
+    cells = math.ceil(N / 4)
+    per_side = math.ceil(round(cells ** (1 / 3), 12))
+    return per_side * ((N / per_side ** 3) / density) ** (1 / 3)
+
+
 def initial_condition(N, temperature, density, seed):
     """engine::InitialCondition: FCC positions, seeded MB velocities (N, 4), box edge."""
     x = np.zeros((N, 4))

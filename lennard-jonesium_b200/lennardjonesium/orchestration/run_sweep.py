@@ -1,14 +1,19 @@
 """run_sweep(): a grid of (temperature, density) simulations, as the reference's
 src/python/lennardjonesium/orchestration/run_sweep.py:37-139 (same arguments,
-folders and per-run config files).  Each simulation runs on the GPU engine;
-thread_count of them run at once (one GPU context per pool worker)."""
+folders and per-run config files).
+
+batched=True (the default) runs every point whose box holds at least 3 cells
+of edge >= cutoff per axis on one batched GPU engine (lj_sim_run_batch: one
+launch per kernel for all systems, CUDA graphs per chunk of steps); the rest,
+and every point when batched=False, run through a SimulationPool of
+thread_count workers, one GPU context each (the reference's parallelism)."""
 
 import os
 import pathlib
 import time
 from copy import deepcopy
 
-from lennardjonesium.simulation import Configuration, Simulation, SimulationPool
+from lennardjonesium.simulation import Configuration, Simulation, SimulationPool, run_batched, fits_batched
 from lennardjonesium.orchestration.results import SweepResult
 from lennardjonesium.orchestration.run import _seed
 from lennardjonesium.orchestration.sweep_configuration import SweepConfiguration
@@ -50,7 +55,7 @@ def _create_simulations(sweep_cfg, random_seed=None, chunk_count=1, chunk_index=
 
 
 def run_sweep(sweep_config_file, echo_status=True, polling_interval=0.5, thread_count=4, random_seed=None,
-              chunk_count=1, chunk_index=0, sweep_config_object=None):
+              chunk_count=1, chunk_index=0, sweep_config_object=None, batched=True):
     """Run every (T, rho) point of the sweep (one chunk of it); returns a SweepResult."""
     path = pathlib.Path(sweep_config_file).resolve()
     if not path.is_file() and sweep_config_object is None:
@@ -65,18 +70,22 @@ def run_sweep(sweep_config_file, echo_status=True, polling_interval=0.5, thread_
     os.chdir(path.parent)
     try:
         sims = _create_simulations(sweep_cfg, random_seed, chunk_count, chunk_index)
-        pool = SimulationPool(thread_count)
+        together = [s for s in sims if batched and fits_batched(s.configuration)]
+        alone = [s for s in sims if not (batched and fits_batched(s.configuration))]
         if echo_status:
-            print(f"==== Lennard-Jones sweep (B200 engine): {len(sims)} runs on {thread_count} threads ====",
-                  flush=True)
+            print(f"==== Lennard-Jones sweep (B200 engine): {len(together)} runs batched, {len(alone)} runs on "
+                  f"{thread_count} threads ====", flush=True)
         t0 = time.perf_counter()
-        for sim in sims:
+        if together:
+            run_batched(together)
+        pool = SimulationPool(thread_count)
+        for sim in alone:
             pool.push(sim)
-        while echo_status:
+        while echo_status and alone:
             st = pool.status()
             print(f"queued {st.waiting}, running {st.running}, completed {st.completed}, "
                   f"{time.perf_counter() - t0:.1f} s", end="\r", flush=True)
-            if st.completed == len(sims):
+            if st.completed == len(alone):
                 print(flush=True)
                 break
             time.sleep(polling_interval)

@@ -74,6 +74,32 @@ class Simulation:
         return self._pair(separation)[2]
 
 
+def run_batched(simulations, echo=False):
+    """Run several Simulations on one batched GPU engine (lj_sim_run_batch): all
+    systems step together, each with its own control protocol and output files.
+    They must share cutoff and time step, and every box edge must be at least
+    3 cutoffs.  Returns the per-simulation results."""
+    if not simulations:
+        return []
+    n = len(simulations)
+    cfgs = (nat.SimConfig * n)(*[_sim_config(sim.configuration) for sim in simulations])
+    res = (nat.SimResult * n)()
+    nat.check(nat.lib().lj_sim_run_batch(cfgs, n, 1 if echo else 0, res))
+    out = []
+    for sim, r in zip(simulations, res):
+        sim.result = {"time_steps": r.time_steps, "outcome": r.outcome, "observations": r.observations,
+                      "seconds": r.seconds}
+        out.append(sim.result)
+    return out
+
+
+def fits_batched(configuration):
+    """True when the run's cubic box holds >= 3 cells of edge >= cutoff per axis."""
+    from lennardjonesium.engine import lattice_side
+    s = configuration.system
+    return lattice_side(s.particle_count, s.density) >= 3 * s.cutoff_distance
+
+
 class SimulationPool:
     """Worker threads that run pushed Simulations (api/simulation_pool.cpp:35-101)."""
 

@@ -1,0 +1,124 @@
+"""The batched engine (lj_batch_*) against single-system runs.
+
+Every block and every cell of the batched launch belongs to one system, the
+rebuilds are gated per system and the reductions follow the single-system
+order, so a batched run must reproduce each system run alone bit for bit.
+"""
+
+import ctypes
+import filecmp
+import pathlib
+
+import numpy as np
+import pytest
+
+import ljref
+
+pytestmark = pytest.mark.gpu
+
+SYSTEMS = [  # N, T, rho, seed: uneven sizes and densities (each box >= 3 cutoffs)
+    (500, 0.5, 0.8, 117208264),
+    (864, 0.722, 0.8442, 5489),
+    (2048, 1.5, 0.3, 3),
+    (4000, 1.2, 0.8, 7),
+    (4 * 9 ** 3, 2.0, 0.05, 11),
+]
+
+
+def _batch(states, L):
+    from lennardjonesium import _native as nat
+    lib = nat.lib()
+    n = len(states)
+    systems = (nat.BatchSystem * n)()
+    for s, ((x, v), box) in enumerate(zip(states, L)):
+        systems[s].particle_count = x.shape[0]
+        for k in range(3):
+            systems[s].box[k] = box
+        systems[s].time_delta = 0.005
+        systems[s].skin = -1.0
+    b = ctypes.c_void_p()
+    nat.check(lib.lj_batch_create(systems, n, 2.5, 0, ctypes.byref(b)))
+    for s, (x, v) in enumerate(states):
+        nat.check(lib.lj_batch_upload_system(b, s, x.ctypes.data_as(ctypes.c_void_p),
+                                             v.ctypes.data_as(ctypes.c_void_p), 4))
+    return lib, b
+
+
+def _download(lib, b, s, N):
+    x, v, F = (np.zeros((N, 4)) for _ in range(3))
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    assert lib.lj_batch_download_system(b, s, P(x), P(v), P(F), 4) == 0
+    return x, v, F
+
+
+def test_batch_equals_single_systems():
+    from lennardjonesium import GpuSystem
+    states, L = [], []
+    for N, T, rho, seed in SYSTEMS:
+        x, v, box = ljref.initial_state(N, T, rho, seed)
+        states.append((x, v))
+        L.append(box)
+    lib, b = _batch(states, L)
+    steps = 203  # graph chunks of 8 plus a remainder
+    recs = np.zeros((steps, len(SYSTEMS), 7))
+    assert lib.lj_batch_step(b, steps, recs.ctypes.data_as(ctypes.c_void_p)) == 0
+    builds = (ctypes.c_longlong * len(SYSTEMS))()
+    lib.lj_batch_info(b, None, builds, None)
+    for s, ((x, v), box) in enumerate(zip(states, L)):
+        with GpuSystem(x.shape[0], box) as g:
+            g.upload(x, v=v)
+            ref = g.step(steps)
+            st = g.download()
+            assert g.stats()["list_builds"] == builds[s]
+        assert np.array_equal(recs[:, s, :], ref), f"system {s}"
+        bx, bv, bF = _download(lib, b, s, x.shape[0])
+        assert np.array_equal(bx, st["x"]) and np.array_equal(bv, st["v"]) and np.array_equal(bF, st["F"])
+    lib.lj_batch_destroy(b)
+
+
+def test_batch_set_temperature_and_inactive():
+    states, L = [], []
+    for N, T, rho, seed in SYSTEMS[:3]:
+        x, v, box = ljref.initial_state(N, T, rho, seed)
+        states.append((x, v))
+        L.append(box)
+    lib, b = _batch(states, L)
+    recs = np.zeros((20, 3, 7))
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    assert lib.lj_batch_step(b, 20, P(recs)) == 0
+    measured = ctypes.c_double()
+    assert lib.lj_batch_set_temperature(b, 1, 1.7, ctypes.byref(measured)) == 0
+    assert measured.value == pytest.approx(recs[-1, 1, 5], rel=1e-14)
+    m = np.zeros((3, 7))
+    assert lib.lj_batch_measure(b, P(m)) == 0
+    assert m[1, 5] == pytest.approx(1.7, rel=1e-14)
+    frozen = _download(lib, b, 2, states[2][0].shape[0])
+    assert lib.lj_batch_set_active(b, 2, 0) == 0
+    assert lib.lj_batch_step(b, 16, P(np.zeros((16, 3, 7)))) == 0
+    after = _download(lib, b, 2, states[2][0].shape[0])
+    assert all(np.array_equal(p, q) for p, q in zip(frozen, after))
+    lib.lj_batch_destroy(b)
+
+
+def test_run_sweep_batched_equals_thread_pool(tmp_path):
+    """The batched sweep writes byte-identical files to the one-context-per-run path."""
+    import lennardjonesium as lj
+    sc = lj.SweepConfiguration()
+    sc.system.temperature_start, sc.system.temperature_stop, sc.system.temperature_steps = 0.7, 1.5, 3
+    sc.system.density_start, sc.system.density_stop, sc.system.density_steps = 0.3, 0.9, 3
+    sc.system.particle_count = 500
+    sc.equilibration.adjustment_interval, sc.equilibration.steady_state_time = 50, 150
+    sc.equilibration.timeout, sc.equilibration.tolerance = 1000, 0.05
+    sc.observation.observation_interval, sc.observation.observation_count = 50, 4
+    sc.observation.tolerance = 0.3
+    runs = {}
+    for mode in ("batched", "pool"):
+        d = tmp_path / mode
+        runs[mode] = lj.run_sweep(d / "sweep.ini", echo_status=False, thread_count=3, random_seed=29,
+                                  sweep_config_object=sc, batched=(mode == "batched"))
+    for t, rho in sc.sweep_range():
+        sub = sc.simulation_dir(t, rho)
+        for name in ("events.log", "thermodynamics.csv", "observations.csv", "snapshots.csv"):
+            a, p = tmp_path / "batched" / sub / name, tmp_path / "pool" / sub / name
+            assert filecmp.cmp(a, p, shallow=False), f"{sub}/{name}"
+    assert len(runs["batched"].completed) == len(runs["pool"].completed)
