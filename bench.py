@@ -251,7 +251,7 @@ def e2e_run(torch, g, x, v, K):
 
 def run_ours(args, ws, rank, local):
     import torch
-    from lennardjonesium import GpuSystem, initial_condition
+    from lennardjonesium import GpuSystem, initial_condition, autotune
     from lennardjonesium import _native as nat
 
     torch.cuda.set_device(local)
@@ -263,8 +263,15 @@ def run_ours(args, ws, rank, local):
     F_alg, C, P = alg_flops_per_atom_step(N_ATOMS, L, WORK["rc"], WORK["rho"])
 
     results = {}
+    tuning = {}
     for prec in ("fp64", "mixed"):
-        g = GpuSystem(N_ATOMS, L, cutoff=WORK["rc"], dt=WORK["dt"], precision=prec, device=local)
+        if args.autotune:
+            kw, tuned_ms = autotune(N_ATOMS, L, x, v, steps=100, cutoff=WORK["rc"], dt=WORK["dt"], precision=prec,
+                                    device=local)
+            tuning[prec] = dict(kw, tuned_ms_per_step=tuned_ms)
+        else:
+            kw = {}
+        g = GpuSystem(N_ATOMS, L, cutoff=WORK["rc"], dt=WORK["dt"], precision=prec, device=local, **kw)
         g.upload(x, v=v)
         g.step_async(args.warmup)
         g.synchronize()
@@ -325,6 +332,7 @@ def run_ours(args, ws, rank, local):
             "phases_ms_per_step": {k: ph[k] / ph["steps"] for k in ("kick_drift_ms", "rebuild_ms", "force_ms",
                                                                      "finalize_ms")},
             "list_builds_per_step": ph["rebuilds"] / ph["steps"],
+            "tuning": tuning or "defaults (skin 0.3, 128 atoms per block)",
             "fma_peaks_tflops": {"fp64": f64.value, "fp32": f32.value}}
     if ws == 1 and rank == 0 and not args.no_cpu_baseline:
         sys.path.insert(0, str(ROOT / "oracle"))
@@ -340,6 +348,93 @@ def run_ours(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+SWEEP = dict(systems=64, T=(0.5, 2.0, 8), rho=(0.05, 1.0, 8), n=(5, 20), rc=2.5, dt=0.005, eq=2000, prod=5000,
+             chunk=200, seed=2024, tol=0.05)
+
+
+def sweep_systems():
+    """an 8 x 8 grid of rho in [0.05, 1.0] and T in [0.5, 2.0]
+    (the reference's linspace, T outer), N = 4 n^3 with n ~ U{5..20} from a fixed seed."""
+    import numpy as np
+    from lennardjonesium import initial_condition
+    from lennardjonesium.tools import linspace
+    rng = np.random.default_rng(SWEEP["seed"])
+    ns = rng.integers(SWEEP["n"][0], SWEEP["n"][1] + 1, size=SWEEP["systems"])
+    out = []
+    for k, (T, rho) in enumerate((t, d) for t in linspace(*SWEEP["T"]) for d in linspace(*SWEEP["rho"])):
+        N = 4 * int(ns[k]) ** 3
+        x, v, L = initial_condition(N, T, rho, SWEEP["seed"] + k)
+        out.append(dict(N=N, T=T, rho=rho, x=x, v=v, L=L))
+    return out
+
+
+def run_sweep_bench(args):
+    """Batched engine vs the same 64 systems run one after another on the GPU: identical
+    protocol in both arms (chunks of 200 steps; during the first 2000 steps a system
+    whose mean T over the chunk is off by >= 5% is rescaled to its target)."""
+    import numpy as np
+    import torch
+    from lennardjonesium import GpuSystem
+    from lennardjonesium import _native as nat
+    systems = sweep_systems()
+    nsys = len(systems)
+    total_steps = SWEEP["eq"] + SWEEP["prod"]
+    chunk = SWEEP["chunk"]
+    lib = nat.lib()
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+
+    # batched
+    table = (nat.BatchSystem * nsys)()
+    for s, sy in enumerate(systems):
+        table[s].particle_count = sy["N"]
+        for k in range(3):
+            table[s].box[k] = sy["L"]
+        table[s].time_delta = SWEEP["dt"]
+        table[s].skin = -1.0
+    b = ctypes.c_void_p()
+    nat.check(lib.lj_batch_create(table, nsys, SWEEP["rc"], 0, ctypes.byref(b)))
+    for s, sy in enumerate(systems):
+        nat.check(lib.lj_batch_upload_system(b, s, P(sy["x"]), P(sy["v"]), 4))
+    recs = np.zeros((chunk, nsys, 7))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for step in range(0, total_steps, chunk):
+        nat.check(lib.lj_batch_step(b, chunk, P(recs)))
+        if step + chunk <= SWEEP["eq"]:
+            for s, sy in enumerate(systems):
+                if abs(recs[:, s, 5].mean() / sy["T"] - 1) >= SWEEP["tol"]:
+                    nat.check(lib.lj_batch_set_temperature(b, s, sy["T"], None))
+    torch.cuda.synchronize()
+    t_batched = time.perf_counter() - t0
+    final_batched = recs[-1].copy()
+    lib.lj_batch_destroy(b)
+
+    # sequential, one context at a time
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    final_seq = np.zeros((nsys, 7))
+    for s, sy in enumerate(systems):
+        with GpuSystem(sy["N"], sy["L"], cutoff=SWEEP["rc"], dt=SWEEP["dt"]) as g:
+            g.upload(sy["x"], v=sy["v"])
+            for step in range(0, total_steps, chunk):
+                r = g.step(chunk)
+                if step + chunk <= SWEEP["eq"] and abs(r[:, 5].mean() / sy["T"] - 1) >= SWEEP["tol"]:
+                    g.set_temperature(sy["T"])
+            final_seq[s] = r[-1]
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    atoms = sum(sy["N"] for sy in systems)
+    line = {"metric": "batched 64-system (T, rho) sweep vs sequential GPU runs", "unit": "atom-steps/s",
+            "value": atoms * total_steps / t_batched, "sequential": atoms * total_steps / t_seq,
+            "speedup": t_seq / t_batched, "seconds_batched": t_batched, "seconds_sequential": t_seq,
+            "systems": nsys, "atoms": atoms, "steps": total_steps,
+            "identical_final_records": bool(np.array_equal(final_batched, final_seq)),
+            "config": {"workload": "8x8 grid rho in [0.05,1.0] x T in [0.5,2.0], N=4n^3, n~U{5..20} (seed 2024), "
+                                   "rc=2.5, dt=0.005, 2000 equilibration + 5000 production steps, FP64",
+                       "timing": "wall clock around synchronised device work (host decisions included)"}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -348,6 +443,10 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--drift-steps", type=int, default=10000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="skip the autotuner (skin and pair-kernel block size per precision)")
+    ap.add_argument("--workload", choices=("single", "sweep"), default="single",
+                    help="single: the 1M-atom benchmark line; sweep: batched vs sequential 64-system sweep")
     ap.add_argument("--cells", type=int, default=64,
                     help="FCC cells per box edge (N = 4 cells^3); 64 is the benchmark workload")
     args = ap.parse_args()
@@ -356,6 +455,9 @@ def main():
     N_ATOMS = 4 * args.cells ** 3
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload == "sweep":
+        run_sweep_bench(args)
+        return
     if args.impl == "reference":
         # CPU only: rank 0 runs the reference arm, the other ranks exit at once
         run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))

@@ -71,6 +71,7 @@ typedef struct lj_params {
     int device;              /* CUDA device ordinal */
     double skin;             /* Verlet-list skin; < 0 selects the default (0.3) */
     int neighbor_capacity;   /* list entries per atom; 0 selects a density-based default */
+    int force_block;         /* atoms per block of the pair kernel: 64, 128 or 256; 0 selects 128 */
 } lj_params;
 
 /* One ThermodynamicMeasurement::Result (physics/measurements.hpp:42-56). */
@@ -184,6 +185,14 @@ typedef struct lj_phase_times {
     long long rebuilds;
 } lj_phase_times;
 int lj_gpu_step_timed(lj_ctx* ctx, int nsteps, lj_phase_times* out);
+
+/* Project autotuner: times `steps` steps of the system described by base and
+ * the state (x, v; N x stride doubles) for each candidate skin (the list-cell
+ * edge rc + skin and the rebuild frequency) and pair-kernel block size (atoms
+ * per block: 64, 128, 256), each in a fresh context from the same state, and
+ * writes the fastest parameters to *best (and its ms per step). */
+int lj_gpu_autotune(const lj_params* base, const double* x, const double* v, int stride, int steps,
+                    lj_params* best, double* best_ms_per_step);
 
 /* Measured FMA throughput of the CUDA-core FP64 and FP32 pipes of a device
  * (TFLOP/s, 2 flops per FMA): the roofline denominators of the pair kernels. */

@@ -346,7 +346,7 @@ b_force_kernel(const int* __restrict__ blk_sys, const int* __restrict__ blk_firs
             unsigned e[4] = {cur.x, cur.y, cur.z, cur.w};
             double4 q[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) q[u] = pos[e[u] & kSlotMask];
+            for (int u = 0; u < 4; ++u) q[u] = ld_pos(pos + (e[u] & kSlotMask));
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 double dx, dy, dz, f, V, W;

@@ -35,7 +35,9 @@ struct lj_ctx {
     Grid list_grid{};
     Grid ref_grid{};
     int cap = 0;
-    int nblocks = 0;
+    int nblocks = 0;      // blocks of kThreads atoms (integration, measurement)
+    int force_block = 128;
+    int fblocks = 0;      // blocks of the pair kernel
     cudaStream_t stream = nullptr;
 
     // device buffers
@@ -218,26 +220,26 @@ int launch_rebuild(lj_ctx* ctx) {
     return LJ_OK;
 }
 
-int launch_force(lj_ctx* ctx, bool kick) {
+template <int BS>
+int launch_force_bs(lj_ctx* ctx, bool kick) {
     int N = ctx->N;
     Soa s = soa_of(ctx->soa, N);
-    dim3 gr(ctx->nblocks), bl(kThreads);
+    dim3 gr(ctx->fblocks), bl(BS);
     int kind = ctx->p.force_kind;
     if (ctx->p.precision == LJ_PRECISION_MIXED && kind == LJ_FORCE_LJ && !ctx->small_box) {
+        MixedParams mp = mixed_params(ctx->pp, ctx->list_grid);
         if (kick)
-            force_mixed_kernel<true><<<gr, bl, 0, ctx->stream>>>(N, ctx->posl, s, ctx->nbr, ctx->cnt,
-                                                                  ctx->pp, mixed_params(ctx->pp, ctx->list_grid),
-                                                                  ctx->partials);
+            force_mixed_kernel<true, BS><<<gr, bl, 0, ctx->stream>>>(N, ctx->posl, s, ctx->nbr, ctx->cnt, ctx->pp, mp,
+                                                                     ctx->partials);
         else
-            force_mixed_kernel<false><<<gr, bl, 0, ctx->stream>>>(N, ctx->posl, s, ctx->nbr, ctx->cnt,
-                                                                   ctx->pp, mixed_params(ctx->pp, ctx->list_grid),
-                                                                   ctx->partials);
+            force_mixed_kernel<false, BS><<<gr, bl, 0, ctx->stream>>>(N, ctx->posl, s, ctx->nbr, ctx->cnt, ctx->pp, mp,
+                                                                      ctx->partials);
         CKL();
         return LJ_OK;
     }
-#define LJ_FORCE_LAUNCH(K, S, KK)                                                                \
-    force_fp64_kernel<K, S, KK><<<gr, bl, 0, ctx->stream>>>(N, ctx->pos, s, ctx->nbr, ctx->cnt, \
-                                                            ctx->pp, ctx->partials)
+#define LJ_FORCE_LAUNCH(K, S, KK)                                                                       \
+    force_fp64_kernel<K, S, KK, BS><<<gr, bl, 0, ctx->stream>>>(N, ctx->pos, s, ctx->nbr, ctx->cnt, \
+                                                                ctx->pp, ctx->partials)
     bool sm = ctx->small_box;
     if (kind == LJ_FORCE_LJ) {
         if (sm) { if (kick) LJ_FORCE_LAUNCH(KIND_LJ, true, true); else LJ_FORCE_LAUNCH(KIND_LJ, true, false); }
@@ -250,6 +252,18 @@ int launch_force(lj_ctx* ctx, bool kick) {
     CKL();
     return LJ_OK;
 }
+
+// Pair kernel at the context's block size (64, 128 or 256 atoms per block).
+int launch_force(lj_ctx* ctx, bool kick) {
+    switch (ctx->force_block) {
+        case 64: return launch_force_bs<64>(ctx, kick);
+        case 256: return launch_force_bs<256>(ctx, kick);
+        default: return launch_force_bs<128>(ctx, kick);
+    }
+}
+
+// Number of partial-sum blocks the last step's measurement pass wrote.
+int partial_blocks(const lj_ctx* ctx, bool forces) { return forces ? ctx->fblocks : ctx->nblocks; }
 
 int launch_kick_drift(lj_ctx* ctx) {
     int N = ctx->N;
@@ -282,7 +296,7 @@ int launch_step(lj_ctx* ctx) {
                                                                          ctx->pp.dt, 1, ctx->partials);
         CKL();
     }
-    finalize_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->partials, ctx->nblocks, ctx->N, ctx->pp.dt, 0,
+    finalize_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->partials, partial_blocks(ctx, forces), ctx->N, ctx->pp.dt, 0,
                                                  forces ? 1 : 0, ctx->sc, ctx->ring, ctx->ring_cap);
     CKL();
     return LJ_OK;
@@ -359,7 +373,8 @@ int build_step_graph(lj_ctx* ctx, int nsteps) {
             if (cudaGetLastError() != cudaSuccess) rc = LJ_ERR_CUDA;
         }
         if (rc) break;
-        finalize_kernel<<<1, 1024, 0, main>>>(ctx->partials, ctx->nblocks, ctx->N, ctx->pp.dt, 0, forces ? 1 : 0,
+        finalize_kernel<<<1, 1024, 0, main>>>(ctx->partials, partial_blocks(ctx, forces), ctx->N, ctx->pp.dt, 0,
+                                              forces ? 1 : 0,
                                               ctx->sc, ctx->ring, ctx->ring_cap);
         if (cudaGetLastError() != cudaSuccess) rc = LJ_ERR_CUDA;
     }
@@ -524,6 +539,12 @@ int lj_gpu_create(const lj_params* params, lj_ctx** out) {
     cap = (std::max(cap, 1) + 3) & ~3;  // whole groups of 4
     ctx->cap = cap;
     ctx->nblocks = blocks_for(N);
+    if (p.force_block != 0 && p.force_block != 64 && p.force_block != 128 && p.force_block != 256) {
+        delete ctx;
+        return LJ_ERR_ARG;
+    }
+    ctx->force_block = p.force_block ? p.force_block : 128;
+    ctx->fblocks = blocks_for(N, ctx->force_block);
 
     int ncl = ctx->list_grid.ncell();
     // slot N is a ghost far outside the box: it pads the last neighbour group
@@ -543,7 +564,7 @@ int lj_gpu_create(const lj_params* params, lj_ctx** out) {
     CK(cudaMalloc(&ctx->tile_sums, sizeof(int) * kMaxScanTiles));
     CK(cudaMalloc(&ctx->nbr, sizeof(uint4) * (size_t)(cap / 4) * N));
     CK(cudaMalloc(&ctx->cnt, sizeof(int) * N));
-    CK(cudaMalloc(&ctx->partials, sizeof(double) * 4 * ctx->nblocks));
+    CK(cudaMalloc(&ctx->partials, sizeof(double) * 4 * std::max(ctx->nblocks, ctx->fblocks)));
     CK(cudaMalloc(&ctx->sc, sizeof(Scalars)));
     ctx->ring_cap = 1024;
     CK(cudaMalloc(&ctx->ring, sizeof(double) * 7 * (ctx->ring_cap + 1)));
@@ -666,7 +687,7 @@ int lj_gpu_compute_forces(lj_ctx* ctx, double* pe, double* virial) {
         if (rc) return rc;
         rc = launch_force(ctx, false);
         if (rc) return rc;
-        finalize_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->partials, ctx->nblocks, ctx->N, ctx->pp.dt, 1, 1,
+        finalize_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->partials, ctx->fblocks, ctx->N, ctx->pp.dt, 1, 1,
                                                      ctx->sc, ctx->ring, ctx->ring_cap);
         CKL();
     }
@@ -897,8 +918,8 @@ int lj_gpu_step_timed(lj_ctx* ctx, int nsteps, lj_phase_times* out) {
             CKL();
         }
         CK(cudaEventRecord(ev[3], ctx->stream));
-        finalize_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->partials, ctx->nblocks, ctx->N, ctx->pp.dt, 0,
-                                                     forces ? 1 : 0, ctx->sc, ctx->ring, ctx->ring_cap);
+        finalize_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->partials, partial_blocks(ctx, forces), ctx->N, ctx->pp.dt,
+                                                     0, forces ? 1 : 0, ctx->sc, ctx->ring, ctx->ring_cap);
         CKL();
         CK(cudaEventRecord(ev[4], ctx->stream));
         CK(cudaEventSynchronize(ev[4]));
@@ -916,6 +937,65 @@ int lj_gpu_step_timed(lj_ctx* ctx, int nsteps, lj_phase_times* out) {
     out->rebuilds = after.builds - before.builds;
     ctx->host_steps += nsteps;
     return read_flags(ctx);
+}
+
+}  // extern "C"
+
+extern "C" {
+
+// Project autotuner: for the caller's system (base params + state), time
+// `steps` velocity-Verlet steps for every candidate (skin, pair-kernel block
+// size) and return the fastest parameters.  The skin sets the list-cell edge
+// rc + skin (the cell-tile shape) and, against it, the rebuild frequency; the
+// block size sets atoms per block and the pair kernel's occupancy.  Each
+// candidate runs in its own context from the same initial state after a
+// warm-up long enough to build the step graph and the first neighbour list.
+int lj_gpu_autotune(const lj_params* base, const double* x, const double* v, int stride, int steps,
+                    lj_params* best, double* best_ms_per_step) {
+    if (!base || !x || !best || steps < 1 || (stride != 3 && stride != 4)) return LJ_ERR_ARG;
+    const double skins[] = {0.15, 0.2, 0.3, 0.4, 0.5};
+    const int blocks[] = {64, 128, 256};
+    double best_ms = 1e300;
+    lj_params winner = *base;
+    double Lmin = std::min(base->box[0], std::min(base->box[1], base->box[2]));
+    double last_skin = -1.0;
+    for (double sk : skins) {
+        double eff = list_skin(sk, Lmin, base->cutoff_distance);
+        if (eff == last_skin) continue;  // the box clips this skin to one already tried
+        last_skin = eff;
+        for (int bs : blocks) {
+            lj_params p = *base;
+            p.skin = sk;
+            p.force_block = bs;
+            lj_ctx* ctx = nullptr;
+            int rc = lj_gpu_create(&p, &ctx);
+            if (rc) return rc;
+            float ms = 0;
+            cudaEvent_t e0 = nullptr, e1 = nullptr;
+            rc = lj_gpu_upload_state(ctx, x, v, nullptr, nullptr, stride, 0.0, 0.0, 0.0);
+            if (!rc) rc = lj_gpu_step_async(ctx, 16);
+            if (!rc) rc = lj_gpu_synchronize(ctx);
+            if (!rc && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)) rc = LJ_ERR_CUDA;
+            if (!rc) {
+                cudaEventRecord(e0, ctx->stream);
+                rc = lj_gpu_step_async(ctx, steps);
+                cudaEventRecord(e1, ctx->stream);
+            }
+            if (!rc) rc = lj_gpu_synchronize(ctx);
+            if (!rc && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) rc = LJ_ERR_CUDA;
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+            lj_gpu_destroy(ctx);
+            if (rc) return rc;
+            if (ms / steps < best_ms) {
+                best_ms = ms / steps;
+                winner = p;
+            }
+        }
+    }
+    *best = winner;
+    if (best_ms_per_step) *best_ms_per_step = best_ms;
+    return LJ_OK;
 }
 
 }  // extern "C"

@@ -444,6 +444,14 @@ build_list_warp_kernel(int N, const double4* __restrict__ pos, const float4* __r
 // ---------------------------------------------------------------------------
 enum { KIND_LJ = 1, KIND_CONST = 2 };
 
+// One 32-byte position in a single 256-bit load (sm_100 ld.global.v4.f64;
+// positions are double4 in cudaMalloc'd arrays, so always 32-byte aligned).
+__device__ __forceinline__ double4 ld_pos(const double4* p) {
+    double4 r;
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(r.x), "=d"(r.y), "=d"(r.z), "=d"(r.w) : "l"(p));
+    return r;
+}
+
 // 1/x: the hardware's approximate FP64 reciprocal refined by two Newton-Raphson
 // steps y <- y + y (1 - x y) (quadratic convergence from the ~2^-20 seed to
 // the last bit of the result).
@@ -499,8 +507,8 @@ __device__ __forceinline__ void pair_fp64(const PairParams& pp, double r2, doubl
     }
 }
 
-template <int KIND, bool SMALL, bool KICK>
-static __global__ void __launch_bounds__(kThreads, 4)
+template <int KIND, bool SMALL, bool KICK, int BS = kThreads>
+static __global__ void __launch_bounds__(BS, 512 / BS)
 force_fp64_kernel(int N, const double4* __restrict__ pos, Soa s, const uint4* __restrict__ nbr4,
                   const int* __restrict__ cnt, PairParams pp, double* __restrict__ partials) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -517,7 +525,7 @@ force_fp64_kernel(int N, const double4* __restrict__ pos, Soa s, const uint4* __
             unsigned e[4] = {cur.x, cur.y, cur.z, cur.w};
             double4 q[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) q[u] = pos[e[u] & kSlotMask];
+            for (int u = 0; u < 4; ++u) q[u] = ld_pos(pos + (e[u] & kSlotMask));
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 double dx, dy, dz, f, V, W;
@@ -548,7 +556,7 @@ force_fp64_kernel(int N, const double4* __restrict__ pos, Soa s, const uint4* __
             }
         }
     }
-    block_sum<4, kThreads>(acc);
+    block_sum<4, BS>(acc);
     if (threadIdx.x == 0)
         for (int q = 0; q < 4; ++q) partials[(size_t)blockIdx.x * 4 + q] = acc[q];
 }

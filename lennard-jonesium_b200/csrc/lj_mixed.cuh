@@ -68,8 +68,8 @@ __device__ __forceinline__ float rcp_approx(float x) {
     return y;
 }
 
-template <bool KICK>
-static __global__ void __launch_bounds__(kThreads, 4)
+template <bool KICK, int BS = kThreads>
+static __global__ void __launch_bounds__(BS, 512 / BS)
 force_mixed_kernel(int N, const float4* __restrict__ posl, Soa s, const uint4* __restrict__ nbr4,
                    const int* __restrict__ cnt, PairParams pp, MixedParams mp,
                    double* __restrict__ partials) {
@@ -145,7 +145,7 @@ force_mixed_kernel(int N, const float4* __restrict__ posl, Soa s, const uint4* _
             }
         }
     }
-    block_sum<4, kThreads>(acc);
+    block_sum<4, BS>(acc);
     if (threadIdx.x == 0)
         for (int q = 0; q < 4; ++q) partials[(size_t)blockIdx.x * 4 + q] = acc[q];
 }

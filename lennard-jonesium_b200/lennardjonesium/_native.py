@@ -29,6 +29,7 @@ class Params(ctypes.Structure):
         ("device", ctypes.c_int),
         ("skin", ctypes.c_double),
         ("neighbor_capacity", ctypes.c_int),
+        ("force_block", ctypes.c_int),
     ]
 
 
@@ -118,6 +119,7 @@ SIGNATURES = {
     "lj_gpu_step_async": (ctypes.c_int, [P, ctypes.c_int]),
     "lj_gpu_synchronize": (ctypes.c_int, [P]),
     "lj_gpu_step_timed": (ctypes.c_int, [P, ctypes.c_int, P]),
+    "lj_gpu_autotune": (ctypes.c_int, [P, P, P, ctypes.c_int, ctypes.c_int, P, P]),
     "lj_gpu_fma_peaks": (ctypes.c_int, [ctypes.c_int, P, P]),
     "lj_gpu_rdf_noalloc": (ctypes.c_int, [P, ctypes.c_int, P, ctypes.c_int, ctypes.c_double, P, P]),
     "lj_sim_run": (ctypes.c_int, [P, ctypes.c_int, P]),

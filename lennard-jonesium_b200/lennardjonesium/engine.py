@@ -50,28 +50,49 @@ def initial_condition(N, temperature, density, seed):
     return x, v, float(side[0])
 
 
+def autotune(N, box, x, v, steps=100, **kw):
+    """Project autotuner (lj_gpu_autotune): the fastest (skin, force_block) for this
+    system and state, as GpuSystem keyword arguments, plus its ms per step."""
+    base = _params(N, box, **kw)
+    best = nat.Params()
+    ms = ctypes.c_double()
+    xs, vs = _as4(x, N), _as4(v, N) if v is not None else None
+    nat.check(nat.lib().lj_gpu_autotune(ctypes.byref(base), _p(xs), _p(vs), 4, int(steps), ctypes.byref(best),
+                                        ctypes.byref(ms)))
+    return {"skin": best.skin, "force_block": best.force_block}, ms.value
+
+
+def _params(N, box, cutoff=2.5, dt=0.005, precision="fp64", force="lj", strength=0.0, periodic=True, device=0,
+            skin=None, capacity=0, force_block=0):
+    L = nat.lib()
+    p = nat.Params()
+    L.lj_gpu_default_params(ctypes.byref(p))
+    p.particle_count = int(N)
+    b = np.broadcast_to(np.asarray(box, dtype=np.float64), (3,))
+    for k in range(3):
+        p.box[k] = float(b[k])
+    p.cutoff_distance = float(cutoff)
+    p.time_delta = float(dt)
+    p.precision = {"fp64": nat.LJ_PRECISION_FP64, "mixed": nat.LJ_PRECISION_MIXED}[precision]
+    p.force_kind = {"none": nat.LJ_FORCE_NONE, "lj": nat.LJ_FORCE_LJ, "constant": nat.LJ_FORCE_CONSTANT}[force]
+    p.force_strength = float(strength)
+    p.periodic = 1 if periodic else 0
+    p.device = int(device)
+    p.skin = -1.0 if skin is None else float(skin)
+    p.neighbor_capacity = int(capacity)
+    p.force_block = int(force_block)
+    return p
+
+
 class GpuSystem:
     """One periodic LJ system resident on a GPU."""
 
     def __init__(self, N, box, cutoff=2.5, dt=0.005, precision="fp64", force="lj", strength=0.0,
-                 periodic=True, device=0, skin=None, capacity=0):
+                 periodic=True, device=0, skin=None, capacity=0, force_block=0):
         L = nat.lib()
-        p = nat.Params()
-        L.lj_gpu_default_params(ctypes.byref(p))
-        p.particle_count = int(N)
+        p = _params(N, box, cutoff=cutoff, dt=dt, precision=precision, force=force, strength=strength,
+                    periodic=periodic, device=device, skin=skin, capacity=capacity, force_block=force_block)
         b = np.broadcast_to(np.asarray(box, dtype=np.float64), (3,))
-        for k in range(3):
-            p.box[k] = float(b[k])
-        p.cutoff_distance = float(cutoff)
-        p.time_delta = float(dt)
-        p.precision = {"fp64": nat.LJ_PRECISION_FP64, "mixed": nat.LJ_PRECISION_MIXED}[precision]
-        p.force_kind = {"none": nat.LJ_FORCE_NONE, "lj": nat.LJ_FORCE_LJ,
-                        "constant": nat.LJ_FORCE_CONSTANT}[force]
-        p.force_strength = float(strength)
-        p.periodic = 1 if periodic else 0
-        p.device = int(device)
-        p.skin = -1.0 if skin is None else float(skin)
-        p.neighbor_capacity = int(capacity)
         self.N = int(N)
         self.box = b.copy()
         self.params = p

@@ -388,3 +388,30 @@ def test_graph_steps_equal_direct_launches(precision):
     for k in ("x", "v", "d", "F"):
         assert np.array_equal(sa[k], sb[k]), k
     assert np.all(np.isfinite(ra))
+
+
+@pytest.mark.parametrize("skin,block,precision", [(0.15, 64, "fp64"), (0.5, 256, "fp64"), (0.4, 64, "mixed")])
+def test_tuning_parameters_keep_parity(skin, block, precision):
+    """Every autotuner candidate computes the same physics: bit-exact pair sets and
+    FP64 forces within the parity tolerance at other skins and block sizes."""
+    N, T, rho, seed, rc = FCC_CASES[3]
+    x, v, L = perturbed_fcc(N, T, rho, seed)
+    with gpu_system(N, L, skin=skin, force_block=block, precision=precision) as g:
+        g.upload(x)
+        assert pair_key(*g.debug_pairs()) == oracle_pair_key(x, L, rc)
+        pe, w = g.compute_forces()
+        F = g.download()["F"]
+        g.upload(x, v=v)
+        th = g.step(50)
+    Fref, pe_ref, w_ref = ljref.forces(x, L, rc)
+    if precision == "fp64":
+        assert_forces(F, Fref, ljref.force_abs_sum(x, L, rc))
+        assert pe == pytest.approx(pe_ref, rel=1e-12)
+    assert np.all(np.isfinite(th))
+
+
+def test_autotune_returns_a_candidate():
+    from lennardjonesium import autotune
+    x, v, L = ljref.initial_state(4000, 1.2, 0.8, 7)
+    kw, ms = autotune(4000, L, x, v, steps=24)
+    assert kw["force_block"] in (64, 128, 256) and 0.0 <= kw["skin"] <= 0.5 and ms > 0
