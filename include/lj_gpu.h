@@ -326,6 +326,48 @@ int lj_batch_set_temperature(lj_batch* batch, int sys, double target, double* me
 /* Totals for tests and tuning: atoms, neighbour-list builds per system, direct kernel launches. */
 int lj_batch_info(const lj_batch* batch, int* total_atoms, long long* builds_per_system, long long* kernel_launches);
 
+/* ------------------------------------------------------------------------
+ * Differentiable NVE: velocity Verlet (integrator.cpp:62-88) over the LJ
+ * spline generalised to an energy scale epsilon and a length scale sigma
+ * (lennard_jones_force.cpp:68-121 is the case epsilon = sigma = 1; the cutoff
+ * is cutoff_sigma * sigma), FP64, with a hand-written discrete adjoint.
+ * The outputs are the time averages over steps 1..M of the total potential
+ * energy and of the virial pressure rho (T + W / 3N) (physics/analyzers.cpp:73-75).
+ * The backward pass runs the reverse velocity-Verlet sweep with one force
+ * Hessian-vector product per step, recomputing each segment of
+ * checkpoint_every steps from a stored checkpoint, and returns the exact
+ * gradient of w_pe * PE_avg + w_p * P_avg with respect to the initial
+ * positions and velocities, epsilon and sigma.  There is no reference
+ * counterpart: the reference has no derivatives.  Every box edge must hold
+ * at least 3 cells of edge cutoff_sigma * sigma.
+ * ------------------------------------------------------------------------ */
+typedef struct lj_adj_params {
+    int particle_count;
+    double box[3];
+    double time_delta;
+    int steps;            /* M >= 1 */
+    int checkpoint_every; /* k >= 1: states kept every k steps, segments recomputed */
+    double epsilon;
+    double sigma;
+    double cutoff_sigma;  /* cutoff in units of sigma (2.5 in the reference's runs) */
+    int device;
+} lj_adj_params;
+
+typedef struct lj_adj_ctx lj_adj_ctx;
+
+int lj_adj_create(const lj_adj_params* params, lj_adj_ctx** out);
+int lj_adj_destroy(lj_adj_ctx* ctx);
+const char* lj_adj_last_error(const lj_adj_ctx* ctx);
+/* New epsilon and sigma for the next forward pass (the cutoff stays cutoff_sigma * sigma). */
+int lj_adj_set_potential(lj_adj_ctx* ctx, double epsilon, double sigma);
+/* Run M steps from (x0, v0) (N x stride doubles): out2 = {PE_avg, P_avg};
+ * series (may be NULL) receives M x 4 doubles {PE, W, KE, P} of states 1..M. */
+int lj_adj_forward(lj_adj_ctx* ctx, const double* x0, const double* v0, int stride, double* out2, double* series);
+/* Gradient of w_pe * PE_avg + w_p * P_avg at the last forward pass.  Any
+ * output pointer may be NULL. */
+int lj_adj_backward(lj_adj_ctx* ctx, double w_pe, double w_p, double* dx0, double* dv0, int stride,
+                    double* depsilon, double* dsigma);
+
 #ifdef __cplusplus
 }
 #endif

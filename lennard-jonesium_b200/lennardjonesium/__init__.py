@@ -10,3 +10,13 @@ GpuSystem exposes that engine directly.
 from lennardjonesium.engine import GpuSystem, initial_condition, autotune, THERMO_FIELDS
 from lennardjonesium.simulation import SeedGenerator, Configuration, Simulation, SimulationPool
 from lennardjonesium.orchestration import run, run_sweep, SweepConfiguration, SweepResult, RunResult
+
+_ADJOINT = ("AdjointNVE", "DifferentiableNVE", "nve_observables")
+
+
+def __getattr__(name):
+    # the differentiable engine imports torch; load it on first use only
+    if name in _ADJOINT:
+        from lennardjonesium import adjoint
+        return getattr(adjoint, name)
+    raise AttributeError(f"module 'lennardjonesium' has no attribute {name!r}")

@@ -85,6 +85,14 @@ class BatchSystem(ctypes.Structure):
                 ("time_delta", ctypes.c_double), ("skin", ctypes.c_double)]
 
 
+class AdjParams(ctypes.Structure):
+    _fields_ = [("particle_count", ctypes.c_int), ("box", ctypes.c_double * 3),
+                ("time_delta", ctypes.c_double), ("steps", ctypes.c_int),
+                ("checkpoint_every", ctypes.c_int), ("epsilon", ctypes.c_double),
+                ("sigma", ctypes.c_double), ("cutoff_sigma", ctypes.c_double),
+                ("device", ctypes.c_int)]
+
+
 class LJError(RuntimeError):
     """A C-ABI call returned a non-zero status."""
 
@@ -136,6 +144,12 @@ SIGNATURES = {
     "lj_batch_measure": (ctypes.c_int, [P, P]),
     "lj_batch_set_temperature": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double, P]),
     "lj_batch_info": (ctypes.c_int, [P, P, P, P]),
+    "lj_adj_create": (ctypes.c_int, [P, P]),
+    "lj_adj_destroy": (ctypes.c_int, [P]),
+    "lj_adj_last_error": (ctypes.c_char_p, [P]),
+    "lj_adj_set_potential": (ctypes.c_int, [P, ctypes.c_double, ctypes.c_double]),
+    "lj_adj_forward": (ctypes.c_int, [P, P, P, ctypes.c_int, P, P]),
+    "lj_adj_backward": (ctypes.c_int, [P, ctypes.c_double, ctypes.c_double, P, P, ctypes.c_int, P, P]),
     "lj_initial_condition": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                             ctypes.c_uint, P, P, P]),
 }
