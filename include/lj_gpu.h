@@ -72,6 +72,13 @@ typedef struct lj_params {
     double skin;             /* Verlet-list skin; < 0 selects the default (0.3) */
     int neighbor_capacity;   /* list entries per atom; 0 selects a density-based default */
     int force_block;         /* atoms per block of the pair kernel: 64, 128 or 256; 0 selects 128 */
+    /* Mixed path only: 0 runs the pair kernel as a neighbour-list gather
+     * from global memory; 1..8 runs it over shared-memory tiles of that many
+     * consecutive list cells of one column.  tile_capacity: the window atoms
+     * a tile stages in shared memory (0 selects a density-based default; a
+     * tile whose window holds more reads from global memory). */
+    int tile_cells;
+    int tile_capacity;
 } lj_params;
 
 /* One ThermodynamicMeasurement::Result (physics/measurements.hpp:42-56). */
@@ -95,6 +102,9 @@ typedef struct lj_stats {
     int small_box;             /* 1: explicit lattice images, rebuilt every step */
     double skin;               /* skin in use (0 in small-box mode) */
     long long kernel_launches; /* kernels this context has launched */
+    int tile_cells;            /* mixed path: cells per shared-memory tile (0: no tiles) */
+    int tile_capacity;         /* mixed path: window atoms one tile stages */
+    int max_staged;            /* mixed path: largest tile window at the last build */
 } lj_stats;
 
 typedef struct lj_ctx lj_ctx;

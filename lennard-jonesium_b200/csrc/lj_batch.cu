@@ -274,7 +274,7 @@ b_build_list_kernel(const int* __restrict__ cell_sys, const SysDev* __restrict__
                     float2 sx = make_float2(xi.x - ia * S.Lf.x, xi.x - ia * S.Lf.x);
                     float2 sy = make_float2(xi.y - ib * S.Lf.y, xi.y - ib * S.Lf.y);
                     float2 sz = make_float2(xi.z - ic * S.Lf.z, xi.z - ic * S.Lf.z);
-                    unsigned code = (unsigned)image_code(a, b, d) << kSlotBits;
+                    unsigned code = offset_code(a, b, d);
                     int js = start[cell], je = start[cell + 1];
                     for (int j0 = js; j0 < je; j0 += 32) {
                         int cntj = min(32, je - j0);
@@ -301,7 +301,7 @@ b_build_list_kernel(const int* __restrict__ cell_sys, const SysDev* __restrict__
                         while (mask) {
                             int t = __ffs(mask) - 1;
                             mask &= mask - 1;
-                            append_entry(grp, n, cap, (unsigned)(j0 + t) | code, nbr4, Ntot, i);
+                            append_entry(grp, n, cap, make_entry((unsigned)(j0 + t), code), nbr4, Ntot, i);
                         }
                     }
                 }
@@ -311,7 +311,7 @@ b_build_list_kernel(const int* __restrict__ cell_sys, const SysDev* __restrict__
             int m = n < cap ? n : cap;
             cnt[i] = m;
             if (m & 3) {
-                for (int k = m & 3; k < 4; ++k) grp[k] = (unsigned)Ntot | (13u << kSlotBits);
+                for (int k = m & 3; k < 4; ++k) grp[k] = make_entry((unsigned)Ntot, kGhostCode);
                 nbr4[(size_t)(m >> 2) * Ntot + i] = make_uint4(grp[0], grp[1], grp[2], grp[3]);
             }
             wmax = max(wmax, n);
@@ -346,7 +346,7 @@ b_force_kernel(const int* __restrict__ blk_sys, const int* __restrict__ blk_firs
             unsigned e[4] = {cur.x, cur.y, cur.z, cur.w};
             double4 q[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) q[u] = ld_pos(pos + (e[u] & kSlotMask));
+            for (int u = 0; u < 4; ++u) q[u] = ld_pos(pos + entry_slot(e[u]));
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 double dx, dy, dz, f, V, W;

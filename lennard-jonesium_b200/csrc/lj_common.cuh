@@ -12,9 +12,13 @@
 namespace ljb {
 
 constexpr int kThreads = 128;             // block size of per-atom kernels
-constexpr unsigned kSlotBits = 27;        // neighbour entry: slot in the low 27 bits
-constexpr unsigned kSlotMask = (1u << kSlotBits) - 1u;
-constexpr int kMaxAtoms = 1 << kSlotBits; // 134M atoms per context
+// Neighbour entry: slot << 6 | offset code, the code holding i + 1 (0, 1, 2)
+// for each axis' offset i in {-1, 0, 1} in 2 bits (x: bits 0-1, y: 2-3, z: 4-5)
+// -- the stencil cell's offset from the home cell, or in small-box lists the
+// lattice image.
+constexpr unsigned kCodeBits = 6;
+constexpr unsigned kGhostCode = 0x15;     // offset (0, 0, 0)
+constexpr int kMaxAtoms = 1 << 26;        // 67M atoms per context
 constexpr int kScanTile = 4096;           // cells per scan tile (1024 threads x 4)
 constexpr int kMaxScanTiles = 1024;
 
@@ -36,6 +40,7 @@ struct Scalars {
     long long builds;              // neighbour-list builds so far
     long long steps;
     long long graph_rebuilds;      // rebuild subgraphs executed by step graphs
+    int max_staged;                // mixed path: largest tile window at the last build
 };
 
 // Physical constants of the pair kernel.
@@ -77,6 +82,19 @@ __device__ __forceinline__ double norm2(double sx, double sy, double sz) {
 __device__ __forceinline__ int image_code(int ix, int iy, int iz) {
     return 9 * (ix + 1) + 3 * (iy + 1) + (iz + 1);
 }
+
+__host__ __device__ __forceinline__ unsigned offset_code(int ix, int iy, int iz) {
+    return (unsigned)(ix + 1) | ((unsigned)(iy + 1) << 2) | ((unsigned)(iz + 1) << 4);
+}
+
+__host__ __device__ __forceinline__ unsigned make_entry(unsigned slot, unsigned code) {
+    return (slot << kCodeBits) | code;
+}
+
+__device__ __forceinline__ unsigned entry_slot(unsigned e) { return e >> kCodeBits; }
+
+// offset of axis k (0, 1, 2) in {-1, 0, 1}
+__device__ __forceinline__ int entry_axis(unsigned e, int k) { return (int)((e >> (2 * k)) & 3u) - 1; }
 
 // ---- reductions ------------------------------------------------------------
 

@@ -22,6 +22,7 @@
 #include "../../include/lj_gpu.h"
 #include "lj_kernels.cuh"
 #include "lj_mixed.cuh"
+#include "lj_tile.cuh"
 
 using namespace ljb;
 
@@ -68,6 +69,13 @@ struct lj_ctx {
     // mixed-precision buffers
     float4* posl = nullptr;
     double* bx = nullptr;  // x at build (unwrapped reference for local coordinates)
+    // shared-memory tiles of the mixed pair kernel (lj_tile.cuh)
+    bool tiles = false;
+    TileGeom tg{};
+    int tile_cells = 0;
+    int tile_blocks = 0;
+    size_t tile_smem = 0;
+    uint4* nbr8 = nullptr;  // 16-bit tile entries, groups of 8
 
     // debug (reference grid) buffers, allocated on first use
     int* dbg_count = nullptr;
@@ -180,7 +188,7 @@ int launch_binning(lj_ctx* ctx, const Grid& g, int* count, int* start, int* tile
 
 // Rebuild chain: bin into the list grid, sort, gather, list.  Every kernel
 // returns at once when the gate is closed.
-int launch_rebuild(lj_ctx* ctx) {
+int launch_rebuild(lj_ctx* ctx, bool tile_format = true) {
     Gate gate = gate_of(ctx);
     int N = ctx->N;
     int rc = launch_binning<true>(ctx, ctx->list_grid, ctx->count, ctx->start, ctx->tile_sums, gate);
@@ -208,6 +216,10 @@ int launch_rebuild(lj_ctx* ctx) {
     if (ctx->small_box)
         build_list_kernel<true><<<blocks_for(N), kThreads, 0, ctx->stream>>>(
             N, ctx->pos, ctx->posf, ctx->list_grid, ctx->start, Lf, cut2, ctx->cap, ctx->nbr, ctx->cnt, ctx->sc, gate);
+    else if (ctx->tiles && tile_format)
+        build_list_tile_kernel<<<blocks_for(ctx->list_grid.ncell(), kBuildWarps), 32 * kBuildWarps, 0, ctx->stream>>>(
+            N, ctx->posf, ctx->list_grid, ctx->start, Lf, cut2, ctx->cap, ctx->tg.nruns, ctx->nbr8, ctx->cnt, ctx->sc,
+            gate);
     else
         build_list_warp_kernel<<<blocks_for(ctx->list_grid.ncell(), kBuildWarps), 32 * kBuildWarps, 0, ctx->stream>>>(
             N, ctx->pos, ctx->posf, ctx->list_grid, ctx->start, Lf, cut2, ctx->cap, ctx->nbr, ctx->cnt, ctx->sc, gate);
@@ -226,6 +238,17 @@ int launch_force_bs(lj_ctx* ctx, bool kick) {
     Soa s = soa_of(ctx->soa, N);
     dim3 gr(ctx->fblocks), bl(BS);
     int kind = ctx->p.force_kind;
+    if (ctx->tiles) {
+        MixedParams mp = mixed_params(ctx->pp, ctx->list_grid);
+        if (kick)
+            force_mixed_tile_kernel<true><<<ctx->tile_blocks, kTileThreads, ctx->tile_smem, ctx->stream>>>(
+                N, ctx->posl, s, ctx->nbr8, ctx->cnt, ctx->start, ctx->list_grid, ctx->tg, ctx->pp, mp, ctx->partials);
+        else
+            force_mixed_tile_kernel<false><<<ctx->tile_blocks, kTileThreads, ctx->tile_smem, ctx->stream>>>(
+                N, ctx->posl, s, ctx->nbr8, ctx->cnt, ctx->start, ctx->list_grid, ctx->tg, ctx->pp, mp, ctx->partials);
+        CKL();
+        return LJ_OK;
+    }
     if (ctx->p.precision == LJ_PRECISION_MIXED && kind == LJ_FORCE_LJ && !ctx->small_box) {
         MixedParams mp = mixed_params(ctx->pp, ctx->list_grid);
         if (kick)
@@ -263,7 +286,9 @@ int launch_force(lj_ctx* ctx, bool kick) {
 }
 
 // Number of partial-sum blocks the last step's measurement pass wrote.
-int partial_blocks(const lj_ctx* ctx, bool forces) { return forces ? ctx->fblocks : ctx->nblocks; }
+int partial_blocks(const lj_ctx* ctx, bool forces) {
+    return forces ? (ctx->tiles ? ctx->tile_blocks : ctx->fblocks) : ctx->nblocks;
+}
 
 int launch_kick_drift(lj_ctx* ctx) {
     int N = ctx->N;
@@ -433,7 +458,7 @@ int read_flags(lj_ctx* ctx) {
 void free_all(lj_ctx* c) {
     void* ptrs[] = {c->posf, c->pos, c->pos_tmp, c->soa, c->soa_tmp, c->bd, c->ids, c->ids_tmp, c->cell_of,
                     c->rank, c->order, c->count, c->start, c->tile_sums, c->nbr, c->cnt, c->partials,
-                    c->sc, c->ring, c->dscratch, c->posl, c->bx, c->dbg_count, c->dbg_start,
+                    c->sc, c->ring, c->dscratch, c->posl, c->bx, c->nbr8, c->dbg_count, c->dbg_start,
                     c->dbg_members, c->dbg_cell_of, c->dbg_tiles};
     for (void* q : ptrs)
         if (q) cudaFree(q);
@@ -536,7 +561,7 @@ int lj_gpu_create(const lj_params* params, lj_ctx** out) {
     double expect = 4.0 / 3.0 * M_PI * cut * cut * cut * std::max(rho, 1.2);
     int cap = p.neighbor_capacity > 0 ? p.neighbor_capacity : (int)std::ceil(1.5 * expect + 32);
     cap = std::min(cap, std::max(N - 1, 1) * 27);
-    cap = (std::max(cap, 1) + 3) & ~3;  // whole groups of 4
+    cap = (std::max(cap, 1) + 7) & ~7;  // whole groups of 4 (FP64 list) and of 8 (tile list)
     ctx->cap = cap;
     ctx->nblocks = blocks_for(N);
     if (p.force_block != 0 && p.force_block != 64 && p.force_block != 128 && p.force_block != 256) {
@@ -545,6 +570,31 @@ int lj_gpu_create(const lj_params* params, lj_ctx** out) {
     }
     ctx->force_block = p.force_block ? p.force_block : 128;
     ctx->fblocks = blocks_for(N, ctx->force_block);
+    if (p.tile_cells < 0 || p.tile_cells > kTileMaxRun || p.tile_capacity < 0 || p.tile_capacity > kTileMaxSmemAtoms) {
+        delete ctx;
+        return LJ_ERR_ARG;
+    }
+    // mixed path over shared-memory tiles: runs of tile_cells list cells per
+    // column (a run plus its two neighbour cells must not wrap onto itself)
+    if (p.precision == LJ_PRECISION_MIXED && p.force_kind == LJ_FORCE_LJ && !ctx->small_box && p.tile_cells > 0) {
+        const Grid& g = ctx->list_grid;
+        int want = p.tile_cells;
+        int nruns = std::max(1, (g.n[2] + want - 1) / want);
+        while ((g.n[2] + nruns - 1) / nruns + 2 > g.n[2]) ++nruns;
+        int run_max = (g.n[2] + nruns - 1) / nruns;
+        double a3 = (p.box[0] / g.n[0]) * (p.box[1] / g.n[1]) * (p.box[2] / g.n[2]);
+        double expect_win = 9.0 * (run_max + 2) * std::max(rho, 0.1) * a3;
+        int tcap = p.tile_capacity ? p.tile_capacity : (int)std::ceil(1.5 * expect_win + 128);
+        tcap = std::min(kTileMaxSmemAtoms, (tcap + 127) & ~127);
+        if (p.tile_capacity) tcap = p.tile_capacity;
+        ctx->tiles = true;
+        ctx->tile_cells = (g.n[2] + nruns - 1) / nruns;
+        ctx->tg.nruns = nruns;
+        ctx->tg.cap = tcap;
+        for (int k = 0; k < 3; ++k) ctx->tg.a[k] = (float)(p.box[k] / g.n[k]);
+        ctx->tile_blocks = g.n[0] * g.n[1] * nruns;
+        ctx->tile_smem = sizeof(float4) * (size_t)(tcap + 1);
+    }
 
     int ncl = ctx->list_grid.ncell();
     // slot N is a ghost far outside the box: it pads the last neighbour group
@@ -564,7 +614,13 @@ int lj_gpu_create(const lj_params* params, lj_ctx** out) {
     CK(cudaMalloc(&ctx->tile_sums, sizeof(int) * kMaxScanTiles));
     CK(cudaMalloc(&ctx->nbr, sizeof(uint4) * (size_t)(cap / 4) * N));
     CK(cudaMalloc(&ctx->cnt, sizeof(int) * N));
-    CK(cudaMalloc(&ctx->partials, sizeof(double) * 4 * std::max(ctx->nblocks, ctx->fblocks)));
+    CK(cudaMalloc(&ctx->partials, sizeof(double) * 4 * std::max(std::max(ctx->nblocks, ctx->fblocks), ctx->tile_blocks)));
+    if (ctx->tiles) {
+        CK(cudaMalloc(&ctx->nbr8, sizeof(uint4) * (size_t)(cap / 8) * N));
+        int smem = (int)ctx->tile_smem;
+        CK(cudaFuncSetAttribute(force_mixed_tile_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        CK(cudaFuncSetAttribute(force_mixed_tile_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    }
     CK(cudaMalloc(&ctx->sc, sizeof(Scalars)));
     ctx->ring_cap = 1024;
     CK(cudaMalloc(&ctx->ring, sizeof(double) * 7 * (ctx->ring_cap + 1)));
@@ -687,7 +743,7 @@ int lj_gpu_compute_forces(lj_ctx* ctx, double* pe, double* virial) {
         if (rc) return rc;
         rc = launch_force(ctx, false);
         if (rc) return rc;
-        finalize_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->partials, ctx->fblocks, ctx->N, ctx->pp.dt, 1, 1,
+        finalize_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->partials, partial_blocks(ctx, true), ctx->N, ctx->pp.dt, 1, 1,
                                                      ctx->sc, ctx->ring, ctx->ring_cap);
         CKL();
     }
@@ -807,8 +863,11 @@ long long lj_gpu_debug_pairs(lj_ctx* ctx, long long cap, int* pi, int* pj, int* 
     int one = 1;
     if (cudaMemcpyAsync(&ctx->sc->need_rebuild, &one, sizeof(int), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
         return -LJ_ERR_CUDA;
-    int rc = launch_rebuild(ctx);
+    int rc = launch_rebuild(ctx, false);  // the slot-indexed list, whatever the pair kernel reads
     if (rc) return -rc;
+    if (ctx->tiles &&  // the tiled kernel's list is now stale: rebuild it before the next step
+        cudaMemcpyAsync(&ctx->sc->need_rebuild, &one, sizeof(int), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+        return -LJ_ERR_CUDA;
     int* di = nullptr; int* dj = nullptr; int* dm = nullptr; double* dr = nullptr;
     unsigned long long* counter = nullptr;
     long long c = cap > 0 ? cap : 1;
@@ -865,6 +924,9 @@ int lj_gpu_get_stats(const lj_ctx* ctx_c, lj_stats* out) {
     // direct launches + kernel nodes executed by step graphs (kick, decide, force,
     // finalize per step, and the rebuild chain each time the conditional opened)
     out->kernel_launches = ctx->launches + 4 * ctx->graph_launched_steps + (long long)ctx->rebuild_kernels * h.graph_rebuilds;
+    out->tile_cells = ctx->tiles ? ctx->tile_cells : 0;
+    out->tile_capacity = ctx->tiles ? ctx->tg.cap : 0;
+    out->max_staged = h.max_staged;
     return LJ_OK;
 }
 
@@ -944,17 +1006,19 @@ int lj_gpu_step_timed(lj_ctx* ctx, int nsteps, lj_phase_times* out) {
 extern "C" {
 
 // Project autotuner: for the caller's system (base params + state), time
-// `steps` velocity-Verlet steps for every candidate (skin, pair-kernel block
-// size) and return the fastest parameters.  The skin sets the list-cell edge
-// rc + skin (the cell-tile shape) and, against it, the rebuild frequency; the
-// block size sets atoms per block and the pair kernel's occupancy.  Each
-// candidate runs in its own context from the same initial state after a
+// `steps` velocity-Verlet steps for every candidate and return the fastest
+// parameters.  Candidates: the Verlet skin, which sets the list-cell edge
+// rc + skin and, against it, the rebuild frequency; and per skin either the
+// pair kernel's block size (atoms per block: 64, 128, 256) and, on the mixed
+// path, also its shared-memory tile variant at 3 or 6 cells per tile.
+// Each candidate runs in its own context from the same initial state after a
 // warm-up long enough to build the step graph and the first neighbour list.
 int lj_gpu_autotune(const lj_params* base, const double* x, const double* v, int stride, int steps,
                     lj_params* best, double* best_ms_per_step) {
     if (!base || !x || !best || steps < 1 || (stride != 3 && stride != 4)) return LJ_ERR_ARG;
     const double skins[] = {0.15, 0.2, 0.3, 0.4, 0.5};
     const int blocks[] = {64, 128, 256};
+    const int tile_shapes[] = {3, 6};
     double best_ms = 1e300;
     lj_params winner = *base;
     double Lmin = std::min(base->box[0], std::min(base->box[1], base->box[2]));
@@ -963,10 +1027,18 @@ int lj_gpu_autotune(const lj_params* base, const double* x, const double* v, int
         double eff = list_skin(sk, Lmin, base->cutoff_distance);
         if (eff == last_skin) continue;  // the box clips this skin to one already tried
         last_skin = eff;
-        for (int bs : blocks) {
+        Grid lg = make_grid(base->box, base->cutoff_distance + eff);
+        bool tiled = base->precision == LJ_PRECISION_MIXED && base->force_kind == LJ_FORCE_LJ &&
+                     std::min(lg.n[0], std::min(lg.n[1], lg.n[2])) >= 3;
+        for (int q = 0; q < (tiled ? 5 : 3); ++q) {
             lj_params p = *base;
             p.skin = sk;
-            p.force_block = bs;
+            if (q < 3) {
+                p.force_block = blocks[q];
+                p.tile_cells = 0;
+            } else {
+                p.tile_cells = tile_shapes[q - 3];
+            }
             lj_ctx* ctx = nullptr;
             int rc = lj_gpu_create(&p, &ctx);
             if (rc) return rc;

@@ -289,8 +289,7 @@ build_list_kernel(int N, const double4* __restrict__ pos, const float4* __restri
                     nc -= ic * g.n[2];
                     int cell = g.flat(na, nb, nc);
                     float sx = ia * Lf.x, sy = ib * Lf.y, sz = ic * Lf.z;
-                    unsigned code = SMALL ? (unsigned)image_code(ia, ib, ic)
-                                          : (unsigned)image_code(a, b, c);
+                    unsigned code = SMALL ? offset_code(ia, ib, ic) : offset_code(a, b, c);
                     int e = start[cell + 1];
                     for (int j = start[cell]; j < e; ++j) {
                         float4 xj = posf[j];
@@ -298,7 +297,7 @@ build_list_kernel(int N, const double4* __restrict__ pos, const float4* __restri
                         float dy = (xi.y - xj.y) - sy;
                         float dz = (xi.z - xj.z) - sz;
                         if (fmaf(dz, dz, fmaf(dy, dy, dx * dx)) < cut2 && j != i) {
-                            if (n < cap) nbr[((size_t)(n >> 2) * N + i) * 4 + (n & 3)] = (unsigned)j | (code << kSlotBits);
+                            if (n < cap) nbr[((size_t)(n >> 2) * N + i) * 4 + (n & 3)] = make_entry((unsigned)j, code);
                             ++n;
                         }
                     }
@@ -308,7 +307,7 @@ build_list_kernel(int N, const double4* __restrict__ pos, const float4* __restri
         int m = n < cap ? n : cap;
         cnt[i] = m;
         for (int k = m; k < ((m + 3) & ~3); ++k)  // ghost padding (code 13: no image, no offset)
-            nbr[((size_t)(k >> 2) * N + i) * 4 + (k & 3)] = (unsigned)N | (13u << kSlotBits);
+            nbr[((size_t)(k >> 2) * N + i) * 4 + (k & 3)] = make_entry((unsigned)N, kGhostCode);
     }
     // block max of n -> sc->max_count; overflow flag
     int m = n;
@@ -378,7 +377,7 @@ build_list_warp_kernel(int N, const double4* __restrict__ pos, const float4* __r
                         float2 sx = make_float2(xi.x - ia * Lf.x, xi.x - ia * Lf.x);
                         float2 sy = make_float2(xi.y - ib * Lf.y, xi.y - ib * Lf.y);
                         float2 sz = make_float2(xi.z - ic * Lf.z, xi.z - ic * Lf.z);
-                        unsigned code = (unsigned)image_code(a, b, d) << kSlotBits;
+                        unsigned code = offset_code(a, b, d);
                         int js = start[cell], je = start[cell + 1];
                         for (int j0 = js; j0 < je; j0 += 32) {
                             int cntj = min(32, je - j0);
@@ -405,7 +404,7 @@ build_list_warp_kernel(int N, const double4* __restrict__ pos, const float4* __r
                             while (mask) {
                                 int t = __ffs(mask) - 1;
                                 mask &= mask - 1;
-                                append_entry(grp, n, cap, (unsigned)(j0 + t) | code, nbr4, N, i);
+                                append_entry(grp, n, cap, make_entry((unsigned)(j0 + t), code), nbr4, N, i);
                             }
                         }
                     }
@@ -415,7 +414,7 @@ build_list_warp_kernel(int N, const double4* __restrict__ pos, const float4* __r
                 int m = n < cap ? n : cap;
                 cnt[i] = m;
                 if (m & 3) {  // pad the last group with the ghost slot
-                    for (int k = m & 3; k < 4; ++k) grp[k] = (unsigned)N | (13u << kSlotBits);
+                    for (int k = m & 3; k < 4; ++k) grp[k] = make_entry((unsigned)N, kGhostCode);
                     nbr4[(size_t)(m >> 2) * N + i] = make_uint4(grp[0], grp[1], grp[2], grp[3]);
                 }
                 wmax = max(wmax, n);
@@ -471,8 +470,7 @@ __device__ __forceinline__ void separation(const double4& xi, const double4& xj,
     dy = __dsub_rn(xi.y, xj.y);
     dz = __dsub_rn(xi.z, xj.z);
     if (SMALL) {
-        int code = (int)(e >> kSlotBits);
-        int ia = code / 9 - 1, ib = (code / 3) % 3 - 1, ic = code % 3 - 1;
+        int ia = entry_axis(e, 0), ib = entry_axis(e, 1), ic = entry_axis(e, 2);
         dx = __dsub_rn(dx, ia * pp.L[0]);
         dy = __dsub_rn(dy, ib * pp.L[1]);
         dz = __dsub_rn(dz, ic * pp.L[2]);
@@ -518,14 +516,19 @@ force_fp64_kernel(int N, const double4* __restrict__ pos, Soa s, const uint4* __
         bool near = !(xi.x >= pp.near_lo && xi.x < pp.near_hi[0] && xi.y >= pp.near_lo &&
                       xi.y < pp.near_hi[1] && xi.z >= pp.near_lo && xi.z < pp.near_hi[2]);
         double fx = 0, fy = 0, fz = 0, pe = 0, w = 0;
+        // list indices stream from HBM: keep three groups of them in flight
         int ng = (cnt[i] + 3) >> 2;
-        uint4 cur = ng > 0 ? __ldcs(&nbr4[i]) : make_uint4(0, 0, 0, 0);
+        const uint4* lp = nbr4 + i;
+        const uint4 z4 = make_uint4(0u, 0u, 0u, 0u);
+        uint4 L0 = ng > 0 ? __ldcs(lp) : z4;
+        uint4 L1 = ng > 1 ? __ldcs(lp + (size_t)N) : z4;
+        uint4 L2 = ng > 2 ? __ldcs(lp + 2 * (size_t)N) : z4;
         for (int g = 0; g < ng; ++g) {
-            uint4 nxt = g + 1 < ng ? __ldcs(&nbr4[(size_t)(g + 1) * N + i]) : cur;
-            unsigned e[4] = {cur.x, cur.y, cur.z, cur.w};
+            uint4 L3 = g + 3 < ng ? __ldcs(lp + (size_t)(g + 3) * N) : z4;
+            unsigned e[4] = {L0.x, L0.y, L0.z, L0.w};
             double4 q[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) q[u] = ld_pos(pos + (e[u] & kSlotMask));
+            for (int u = 0; u < 4; ++u) q[u] = ld_pos(pos + entry_slot(e[u]));
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 double dx, dy, dz, f, V, W;
@@ -537,7 +540,9 @@ force_fp64_kernel(int N, const double4* __restrict__ pos, Soa s, const uint4* __
                 pe += V;
                 w += W;
             }
-            cur = nxt;
+            L0 = L1;
+            L1 = L2;
+            L2 = L3;
         }
         s.at(FX, i) = fx;
         s.at(FY, i) = fy;
@@ -708,14 +713,13 @@ static __global__ void debug_pairs_kernel(int N, const double4* __restrict__ pos
     const unsigned* nbr = reinterpret_cast<const unsigned*>(nbr4);
     for (int k = 0; k < cnt[i]; ++k) {
         unsigned e = nbr[((size_t)(k >> 2) * N + i) * 4 + (k & 3)];
-        int j = (int)(e & kSlotMask);
+        int j = (int)entry_slot(e);
         if (ids[i] >= ids[j]) continue;
         double4 xj = pos[j];
         double d[3] = {__dsub_rn(xi.x, xj.x), __dsub_rn(xi.y, xj.y), __dsub_rn(xi.z, xj.z)};
         int img[3] = {0, 0, 0};
         if (SMALL) {
-            int code = (int)(e >> kSlotBits);
-            img[0] = code / 9 - 1; img[1] = (code / 3) % 3 - 1; img[2] = code % 3 - 1;
+            for (int q = 0; q < 3; ++q) img[q] = entry_axis(e, q);
         } else {
             for (int q = 0; q < 3; ++q)
                 if ((__double2hiint(d[q]) & 0x7fffffff) > pp.halfL_hi[q]) img[q] = d[q] > 0 ? 1 : -1;

@@ -68,65 +68,81 @@ __device__ __forceinline__ float rcp_approx(float x) {
     return y;
 }
 
+// The 4 neighbour positions of one list group.
+__device__ __forceinline__ void gather4(const float4* __restrict__ posl, const uint4 grp, float4 (&q)[4]) {
+    q[0] = posl[entry_slot(grp.x)];
+    q[1] = posl[entry_slot(grp.y)];
+    q[2] = posl[entry_slot(grp.z)];
+    q[3] = posl[entry_slot(grp.w)];
+}
+
+// Stencil offset of one axis from its 2-bit code c = i + 1: the FP32 value
+// 2^23 + c (exact), so that subtracting 2^23 + 1 gives i in {-1, 0, 1} exactly.
+__device__ __forceinline__ float code_bias(unsigned bits) { return __uint_as_float(0x4b000000u | (bits & 3u)); }
+
 template <bool KICK, int BS = kThreads>
 static __global__ void __launch_bounds__(BS, 512 / BS)
 force_mixed_kernel(int N, const float4* __restrict__ posl, Soa s, const uint4* __restrict__ nbr4,
                    const int* __restrict__ cnt, PairParams pp, MixedParams mp,
                    double* __restrict__ partials) {
-    __shared__ float4 off[27];
-    if (threadIdx.x < 27) {
-        int c = threadIdx.x;
-        off[c] = make_float4((float)(c / 9 - 1) * mp.a[0], (float)((c / 3) % 3 - 1) * mp.a[1],
-                             (float)(c % 3 - 1) * mp.a[2], 0.f);
-    }
-    __syncthreads();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double acc[4] = {0, 0, 0, 0};
+    const float2 na_xy = make_float2(-mp.a[0], -mp.a[1]);
+    const float az = mp.a[2];
+    const float2 unbias = make_float2(-8388609.0f, -8388609.0f);
     if (i < N) {
         const float4 xi = posl[i];
+        const float2 xi_xy = make_float2(xi.x, xi.y);
         double fx = 0, fy = 0, fz = 0, pe = 0, w = 0;
+        // list indices stream from HBM: keep three groups of them in flight
+        // (the neighbour positions, mostly L1/L2 hits, are gathered per group)
         int ng = (cnt[i] + 3) >> 2;
-        uint4 cur = ng > 0 ? __ldcs(&nbr4[i]) : make_uint4(0, 0, 0, 0);
-        for (int g0 = 0; g0 < ng; g0 += 2) {
-            // one chunk = 2 groups = 8 neighbours summed in FP32, then added in FP64
-            float cx = 0.f, cy = 0.f, cz = 0.f, cv = 0.f, cw = 0.f;
+        const uint4* lp = nbr4 + i;
+        const uint4 z4 = make_uint4(0u, 0u, 0u, 0u);
+        uint4 L0 = ng > 0 ? __ldcs(lp) : z4;
+        uint4 L1 = ng > 1 ? __ldcs(lp + (size_t)N) : z4;
+        uint4 L2 = ng > 2 ? __ldcs(lp + 2 * (size_t)N) : z4;
+        // chunks of 2 groups = 8 neighbours summed in FP32, then added in FP64
+        float cx = 0.f, cy = 0.f, cz = 0.f, cv = 0.f, cw = 0.f;
+        for (int g = 0; g < ng; ++g) {
+            uint4 L3 = g + 3 < ng ? __ldcs(lp + (size_t)(g + 3) * N) : z4;
+            float4 Q[4];
+            gather4(posl, L0, Q);
+            const unsigned e[4] = {L0.x, L0.y, L0.z, L0.w};
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                int g = g0 + h;
-                if (g < ng) {
-                    uint4 nxt = g + 1 < ng ? __ldcs(&nbr4[(size_t)(g + 1) * N + i]) : cur;
-                    unsigned e[4] = {cur.x, cur.y, cur.z, cur.w};
-                    float4 q[4];
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) q[u] = posl[e[u] & kSlotMask];
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        float4 o = off[e[u] >> kSlotBits];
-                        float dx = (xi.x - q[u].x) - o.x;
-                        float dy = (xi.y - q[u].y) - o.y;
-                        float dz = (xi.z - q[u].z) - o.z;
-                        float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                        bool hit = r2 < mp.rc2;
-                        float ir2 = rcp_approx(r2);
-                        float ir6 = ir2 * ir2 * ir2;
-                        float x = r2 * mp.inv_rc2;
-                        float V = fmaf(4.f * ir6, ir6 - 1.f, fmaf(mp.beta, x - 1.f, mp.alpha));
-                        float W = fmaf(24.f * ir6, fmaf(2.f, ir6, -1.f), -2.f * mp.beta * x);
-                        float f = hit ? W * ir2 : 0.f;
-                        cx = fmaf(f, dx, cx);
-                        cy = fmaf(f, dy, cy);
-                        cz = fmaf(f, dz, cz);
-                        cv += hit ? V : 0.f;
-                        cw += hit ? W : 0.f;
-                    }
-                    cur = nxt;
-                }
+            for (int u = 0; u < 4; ++u) {
+                // s = (xl_i - xl_j) - offset * a, the offset product exact
+                float2 t_xy = __fadd2_rn(make_float2(code_bias(e[u]), code_bias(e[u] >> 2)), unbias);
+                float tz = code_bias(e[u] >> 4) - 8388609.0f;
+                float2 d_xy = __fadd2_rn(xi_xy, make_float2(-Q[u].x, -Q[u].y));
+                d_xy = __ffma2_rn(t_xy, na_xy, d_xy);
+                float dx = d_xy.x, dy = d_xy.y;
+                float dz = fmaf(-tz, az, xi.z - Q[u].z);
+                float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                bool hit = r2 < mp.rc2;
+                float ir2 = rcp_approx(r2);
+                float ir6 = ir2 * ir2 * ir2;
+                float x = r2 * mp.inv_rc2;
+                float V = fmaf(4.f * ir6, ir6 - 1.f, fmaf(mp.beta, x - 1.f, mp.alpha));
+                float W = fmaf(24.f * ir6, fmaf(2.f, ir6, -1.f), -2.f * mp.beta * x);
+                float f = hit ? W * ir2 : 0.f;
+                cx = fmaf(f, dx, cx);
+                cy = fmaf(f, dy, cy);
+                cz = fmaf(f, dz, cz);
+                cv += hit ? V : 0.f;
+                cw += hit ? W : 0.f;
             }
-            fx += (double)cx;
-            fy += (double)cy;
-            fz += (double)cz;
-            pe += (double)cv;
-            w += (double)cw;
+            if ((g & 1) || g + 1 == ng) {
+                fx += (double)cx;
+                fy += (double)cy;
+                fz += (double)cz;
+                pe += (double)cv;
+                w += (double)cw;
+                cx = cy = cz = cv = cw = 0.f;
+            }
+            L0 = L1;
+            L1 = L2;
+            L2 = L3;
         }
         s.at(FX, i) = fx;
         s.at(FY, i) = fy;

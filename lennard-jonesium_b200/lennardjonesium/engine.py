@@ -51,7 +51,8 @@ def initial_condition(N, temperature, density, seed):
 
 
 def autotune(N, box, x, v, steps=100, **kw):
-    """Project autotuner (lj_gpu_autotune): the fastest (skin, force_block) for this
+    """Project autotuner (lj_gpu_autotune): the fastest (skin, force_block) -- or,
+    on the mixed path's shared-memory tiles, (skin, tile_cells) -- for this
     system and state, as GpuSystem keyword arguments, plus its ms per step."""
     base = _params(N, box, **kw)
     best = nat.Params()
@@ -59,11 +60,11 @@ def autotune(N, box, x, v, steps=100, **kw):
     xs, vs = _as4(x, N), _as4(v, N) if v is not None else None
     nat.check(nat.lib().lj_gpu_autotune(ctypes.byref(base), _p(xs), _p(vs), 4, int(steps), ctypes.byref(best),
                                         ctypes.byref(ms)))
-    return {"skin": best.skin, "force_block": best.force_block}, ms.value
+    return {"skin": best.skin, "force_block": best.force_block, "tile_cells": best.tile_cells}, ms.value
 
 
 def _params(N, box, cutoff=2.5, dt=0.005, precision="fp64", force="lj", strength=0.0, periodic=True, device=0,
-            skin=None, capacity=0, force_block=0):
+            skin=None, capacity=0, force_block=0, tile_cells=0, tile_capacity=0):
     L = nat.lib()
     p = nat.Params()
     L.lj_gpu_default_params(ctypes.byref(p))
@@ -81,6 +82,8 @@ def _params(N, box, cutoff=2.5, dt=0.005, precision="fp64", force="lj", strength
     p.skin = -1.0 if skin is None else float(skin)
     p.neighbor_capacity = int(capacity)
     p.force_block = int(force_block)
+    p.tile_cells = int(tile_cells)
+    p.tile_capacity = int(tile_capacity)
     return p
 
 
@@ -88,10 +91,11 @@ class GpuSystem:
     """One periodic LJ system resident on a GPU."""
 
     def __init__(self, N, box, cutoff=2.5, dt=0.005, precision="fp64", force="lj", strength=0.0,
-                 periodic=True, device=0, skin=None, capacity=0, force_block=0):
+                 periodic=True, device=0, skin=None, capacity=0, force_block=0, tile_cells=0, tile_capacity=0):
         L = nat.lib()
         p = _params(N, box, cutoff=cutoff, dt=dt, precision=precision, force=force, strength=strength,
-                    periodic=periodic, device=device, skin=skin, capacity=capacity, force_block=force_block)
+                    periodic=periodic, device=device, skin=skin, capacity=capacity, force_block=force_block,
+                    tile_cells=tile_cells, tile_capacity=tile_capacity)
         b = np.broadcast_to(np.asarray(box, dtype=np.float64), (3,))
         self.N = int(N)
         self.box = b.copy()
