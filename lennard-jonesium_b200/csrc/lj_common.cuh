@@ -33,6 +33,7 @@ struct Grid {
 struct Scalars {
     double t, pe, vir;
     unsigned long long max_disp2;  // bits of a non-negative double: max |d - d_build|^2 this step
+    unsigned long long max_disp2_next;  // the same for the next step, from a fused pair-kernel epilogue
     int need_rebuild;              // set by the host (upload, forced rebuild)
     int overflow;                  // a neighbour list overflowed
     int nonfinite;                 // a non-finite energy or virial was seen

@@ -66,6 +66,10 @@ struct lj_ctx {
     int ring_cap = 0;
     double* host_ring = nullptr;  // pinned
 
+    // second position buffers: a step graph's fused pair kernels write the next
+    // step's positions here while this step's are still being read
+    double4* pos_b = nullptr;
+    float4* posl_b = nullptr;
     // mixed-precision buffers
     float4* posl = nullptr;
     double* bx = nullptr;  // x at build (unwrapped reference for local coordinates)
@@ -233,7 +237,7 @@ int launch_rebuild(lj_ctx* ctx, bool tile_format = true) {
 }
 
 template <int BS>
-int launch_force_bs(lj_ctx* ctx, bool kick) {
+int launch_force_bs(lj_ctx* ctx, bool kick, const Fuse& fz) {
     int N = ctx->N;
     Soa s = soa_of(ctx->soa, N);
     dim3 gr(ctx->fblocks), bl(BS);
@@ -253,16 +257,16 @@ int launch_force_bs(lj_ctx* ctx, bool kick) {
         MixedParams mp = mixed_params(ctx->pp, ctx->list_grid);
         if (kick)
             force_mixed_kernel<true, BS><<<gr, bl, 0, ctx->stream>>>(N, ctx->posl, s, ctx->nbr, ctx->cnt, ctx->pp, mp,
-                                                                     ctx->partials);
+                                                                     ctx->partials, fz);
         else
             force_mixed_kernel<false, BS><<<gr, bl, 0, ctx->stream>>>(N, ctx->posl, s, ctx->nbr, ctx->cnt, ctx->pp, mp,
-                                                                      ctx->partials);
+                                                                      ctx->partials, fz);
         CKL();
         return LJ_OK;
     }
 #define LJ_FORCE_LAUNCH(K, S, KK)                                                                       \
     force_fp64_kernel<K, S, KK, BS><<<gr, bl, 0, ctx->stream>>>(N, ctx->pos, s, ctx->nbr, ctx->cnt, \
-                                                                ctx->pp, ctx->partials)
+                                                                ctx->pp, ctx->partials, fz)
     bool sm = ctx->small_box;
     if (kind == LJ_FORCE_LJ) {
         if (sm) { if (kick) LJ_FORCE_LAUNCH(KIND_LJ, true, true); else LJ_FORCE_LAUNCH(KIND_LJ, true, false); }
@@ -276,12 +280,30 @@ int launch_force_bs(lj_ctx* ctx, bool kick) {
     return LJ_OK;
 }
 
+// Whether a pair kernel can carry the next step's kick and drift (the
+// neighbour-list kernels with a second kick; not the shared-memory tiles).
+bool can_fuse(const lj_ctx* ctx) { return ctx->p.force_kind != LJ_FORCE_NONE && !ctx->tiles; }
+
 // Pair kernel at the context's block size (64, 128 or 256 atoms per block).
-int launch_force(lj_ctx* ctx, bool kick) {
+// With pos_next / posl_next it also runs the next step's first half kick and
+// drift, writing the new positions there.
+int launch_force(lj_ctx* ctx, bool kick, double4* pos_next = nullptr, float4* posl_next = nullptr) {
+    Fuse fz{};
+    if (kick && pos_next) {
+        fz.pos_next = pos_next;
+        fz.posl_next = posl_next;
+        fz.pos = ctx->pos;
+        fz.bd = ctx->bd;
+        fz.bx = ctx->bx;
+        fz.sc = ctx->sc;
+        fz.track = !ctx->rebuild_always;
+        fz.local = ctx->p.precision == LJ_PRECISION_MIXED && ctx->p.force_kind == LJ_FORCE_LJ && !ctx->small_box;
+        fz.periodic = ctx->p.periodic;
+    }
     switch (ctx->force_block) {
-        case 64: return launch_force_bs<64>(ctx, kick);
-        case 256: return launch_force_bs<256>(ctx, kick);
-        default: return launch_force_bs<128>(ctx, kick);
+        case 64: return launch_force_bs<64>(ctx, kick, fz);
+        case 256: return launch_force_bs<256>(ctx, kick, fz);
+        default: return launch_force_bs<128>(ctx, kick, fz);
     }
 }
 
@@ -290,14 +312,15 @@ int partial_blocks(const lj_ctx* ctx, bool forces) {
     return forces ? (ctx->tiles ? ctx->tile_blocks : ctx->fblocks) : ctx->nblocks;
 }
 
-int launch_kick_drift(lj_ctx* ctx) {
+int launch_kick_drift(lj_ctx* ctx, double4* pos_out = nullptr, float4* posl_out = nullptr) {
     int N = ctx->N;
     bool track = !ctx->rebuild_always && ctx->p.force_kind != LJ_FORCE_NONE;
     bool local = ctx->p.precision == LJ_PRECISION_MIXED && ctx->p.force_kind == LJ_FORCE_LJ && !ctx->small_box;
     Soa s = soa_of(ctx->soa, N);
     dim3 gr(ctx->nblocks), bl(kThreads);
 #define LJ_KD(P, T, Lc) \
-    kick_drift_kernel<P, T, Lc><<<gr, bl, 0, ctx->stream>>>(N, ctx->pos, s, ctx->bd, ctx->bx, ctx->posl, ctx->pp, ctx->sc)
+    kick_drift_kernel<P, T, Lc><<<gr, bl, 0, ctx->stream>>>(N, ctx->pos, pos_out ? pos_out : ctx->pos, s, ctx->bd, \
+                                                            ctx->bx, posl_out ? posl_out : ctx->posl, ctx->pp, ctx->sc)
     if (!ctx->p.periodic) LJ_KD(false, false, false);
     else if (local) { if (track) LJ_KD(true, true, true); else LJ_KD(true, false, true); }
     else { if (track) LJ_KD(true, true, false); else LJ_KD(true, false, false); }
@@ -331,6 +354,10 @@ int launch_step(lj_ctx* ctx) {
 //   kick_drift -> decide -> IF(rebuild chain) -> force(+kick) -> finalize
 // where `decide` sets the conditional from the device-side gate, so the
 // rebuild kernels are not even launched on the steps that do not need them.
+// With an even step count the pair kernels of all but the last step also run
+// the next step's kick and drift (Fuse), alternating between the two position
+// buffers: kick_drift only opens the graph (writing the second buffer) and the
+// last, unfused step leaves the state in the first buffer again.
 // Returns LJ_OK with ctx->graph_k set, or an error (the caller then keeps
 // launching the steps one kernel at a time).
 int build_step_graph(lj_ctx* ctx, int nsteps) {
@@ -341,8 +368,21 @@ int build_step_graph(lj_ctx* ctx, int nsteps) {
     if (e != cudaSuccess) return set_err(ctx, LJ_ERR_CUDA, cudaGetErrorString(e));
     int rc = LJ_OK;
     bool forces = ctx->p.force_kind != LJ_FORCE_NONE;
+    bool fuse = forces && can_fuse(ctx) && nsteps % 2 == 0;
+    double4* const posA = ctx->pos;
+    float4* const poslA = ctx->posl;
+    auto other = [&](double4*& x, float4*& xl) {
+        x = ctx->pos == posA ? ctx->pos_b : posA;
+        xl = ctx->posl == poslA ? ctx->posl_b : poslA;
+    };
     for (int st = 0; st < nsteps && rc == LJ_OK; ++st) {
-        rc = launch_kick_drift(ctx);
+        if (!fuse) {
+            rc = launch_kick_drift(ctx);
+        } else if (st == 0) {
+            rc = launch_kick_drift(ctx, ctx->pos_b, ctx->posl_b);
+            ctx->pos = ctx->pos_b;
+            ctx->posl = ctx->posl_b;
+        }
         if (rc) break;
         if (forces) {
             cudaStreamCaptureStatus cs;
@@ -391,7 +431,14 @@ int build_step_graph(lj_ctx* ctx, int nsteps) {
                 rc = LJ_ERR_CUDA;
             }
             if (rc) break;
-            rc = launch_force(ctx, true);
+            if (fuse && st + 1 < nsteps) {
+                double4* nx = nullptr;
+                float4* nxl = nullptr;
+                other(nx, nxl);
+                rc = launch_force(ctx, true, nx, nxl);
+            } else {
+                rc = launch_force(ctx, true);
+            }
         } else {
             kick_measure_kernel<<<ctx->nblocks, kThreads, 0, main>>>(ctx->N, soa_of(ctx->soa, ctx->N), ctx->pp.dt, 1,
                                                                      ctx->partials);
@@ -402,7 +449,17 @@ int build_step_graph(lj_ctx* ctx, int nsteps) {
                                               forces ? 1 : 0,
                                               ctx->sc, ctx->ring, ctx->ring_cap);
         if (cudaGetLastError() != cudaSuccess) rc = LJ_ERR_CUDA;
+        if (fuse && st + 1 < nsteps) {
+            double4* nx = nullptr;
+            float4* nxl = nullptr;
+            other(nx, nxl);
+            ctx->pos = nx;
+            ctx->posl = nxl;
+        }
     }
+    if (fuse && rc == LJ_OK && ctx->pos != posA) rc = set_err(ctx, LJ_ERR_CUDA, "step graph: buffer parity");
+    ctx->pos = posA;
+    ctx->posl = poslA;
     ctx->stream = main;
     cudaError_t ee = cudaStreamEndCapture(main, &graph);
     ctx->launches = launches0;  // captured launches are not executions
@@ -458,7 +515,8 @@ int read_flags(lj_ctx* ctx) {
 void free_all(lj_ctx* c) {
     void* ptrs[] = {c->posf, c->pos, c->pos_tmp, c->soa, c->soa_tmp, c->bd, c->ids, c->ids_tmp, c->cell_of,
                     c->rank, c->order, c->count, c->start, c->tile_sums, c->nbr, c->cnt, c->partials,
-                    c->sc, c->ring, c->dscratch, c->posl, c->bx, c->nbr8, c->dbg_count, c->dbg_start,
+                    c->sc, c->ring, c->dscratch, c->posl, c->bx, c->nbr8, c->pos_b, c->posl_b, c->dbg_count,
+                    c->dbg_start,
                     c->dbg_members, c->dbg_cell_of, c->dbg_tiles};
     for (void* q : ptrs)
         if (q) cudaFree(q);
@@ -599,6 +657,7 @@ int lj_gpu_create(const lj_params* params, lj_ctx** out) {
     int ncl = ctx->list_grid.ncell();
     // slot N is a ghost far outside the box: it pads the last neighbour group
     CK(cudaMalloc(&ctx->pos, sizeof(double4) * (N + 1)));
+    CK(cudaMalloc(&ctx->pos_b, sizeof(double4) * (N + 1)));
     CK(cudaMalloc(&ctx->posf, sizeof(float4) * (N + 1)));
     CK(cudaMalloc(&ctx->pos_tmp, sizeof(double4) * N));
     CK(cudaMalloc(&ctx->soa, sizeof(double) * SOA_FIELDS * N));
@@ -629,10 +688,12 @@ int lj_gpu_create(const lj_params* params, lj_ctx** out) {
     CK(cudaMallocHost(&ctx->host_ring, sizeof(double) * 7 * ctx->ring_cap));
     if (p.precision == LJ_PRECISION_MIXED) {
         CK(cudaMalloc(&ctx->posl, sizeof(float4) * (N + 1)));
+        CK(cudaMalloc(&ctx->posl_b, sizeof(float4) * (N + 1)));
         CK(cudaMalloc(&ctx->bx, sizeof(double) * 3 * N));
         CK(cudaMemsetAsync(ctx->posl, 0, sizeof(float4) * N, ctx->stream));
         float4 gl = make_float4(1e18f, 1e18f, 1e18f, 0.f);
         CK(cudaMemcpyAsync(ctx->posl + N, &gl, sizeof gl, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->posl_b + N, &gl, sizeof gl, cudaMemcpyHostToDevice, ctx->stream));
         CK(cudaMemsetAsync(ctx->bx, 0, sizeof(double) * 3 * N, ctx->stream));
     }
     CK(cudaMemsetAsync(ctx->pos, 0, sizeof(double4) * N, ctx->stream));
@@ -640,6 +701,7 @@ int lj_gpu_create(const lj_params* params, lj_ctx** out) {
     static const double4 ghost = make_double4(1e18, 1e18, 1e18, 0.0);
     static const float4 ghostf = make_float4(1e18f, 1e18f, 1e18f, 0.f);
     CK(cudaMemcpyAsync(ctx->pos + N, &ghost, sizeof ghost, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->pos_b + N, &ghost, sizeof ghost, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->posf + N, &ghostf, sizeof ghostf, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemsetAsync(ctx->soa, 0, sizeof(double) * SOA_FIELDS * N, ctx->stream));
     CK(cudaMemsetAsync(ctx->bd, 0, sizeof(double) * 3 * N, ctx->stream));

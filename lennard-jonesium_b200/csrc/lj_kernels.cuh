@@ -40,7 +40,7 @@ struct Gate {
 // ---------------------------------------------------------------------------
 template <bool PERIODIC, bool TRACK, bool LOCAL>
 static __global__ void __launch_bounds__(kThreads)
-kick_drift_kernel(int N, double4* __restrict__ pos, Soa s, const double* __restrict__ bd,
+kick_drift_kernel(int N, const double4* pos, double4* pos_out, Soa s, const double* __restrict__ bd,
                   const double* __restrict__ bx, float4* __restrict__ posl, PairParams pp, Scalars* sc) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double m = 0.0;
@@ -65,7 +65,7 @@ kick_drift_kernel(int N, double4* __restrict__ pos, Soa s, const double* __restr
                 if (LOCAL) l[k] = (float)(bx[(size_t)k * N + i] + e);
             }
         }
-        pos[i] = make_double4(xs[0], xs[1], xs[2], 0.0);
+        pos_out[i] = make_double4(xs[0], xs[1], xs[2], 0.0);
         if (LOCAL) posl[i] = make_float4(l[0], l[1], l[2], 0.f);
     }
     if (TRACK) {
@@ -443,6 +443,66 @@ build_list_warp_kernel(int N, const double4* __restrict__ pos, const float4* __r
 // ---------------------------------------------------------------------------
 enum { KIND_LJ = 1, KIND_CONST = 2 };
 
+// Fusion of the next step's first half kick and drift into the pair kernel's
+// epilogue (kick_drift_kernel's arithmetic, in the same order): the new
+// positions go to the other position buffer, which no pair kernel of this
+// step reads.
+struct Fuse {
+    double4* pos_next;        // nullptr: no fusion
+    float4* posl_next;        // mixed path: next step's cell-local coordinates
+    const double4* pos;       // this step's positions (the mixed kernel reads FP32 copies)
+    const double* bd;         // displacement at the last list build
+    const double* bx;         // mixed path: cell-local position at the last list build
+    Scalars* sc;
+    int track, local, periodic;
+};
+
+// Second half kick (integrator.cpp:82) with the measurement partials and, when
+// fused, the next step's first half kick, drift, displacement and periodic
+// wrap (integrator.cpp:70-78).  Returns |d - d_build|^2 for the rebuild test.
+__device__ __forceinline__ double step_epilogue(int N, int i, Soa s, const double4 x, const double (&f3)[3],
+                                                const PairParams& pp, const Fuse& fz, double (&acc)[4]) {
+    double xs[3] = {x.x, x.y, x.z};
+    float l[3] = {0.f, 0.f, 0.f};
+    double m = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        double v = kick(s.at(VX + k, i), f3[k], pp.dt);
+        acc[0] = fma(v, v, acc[0]);
+        double d = s.at(DX + k, i);
+        acc[3] = fma(d, d, acc[3]);
+        if (fz.pos_next) {
+            v = kick(v, f3[k], pp.dt);
+            double inc = __dmul_rn(v, pp.dt);
+            double xn = __dadd_rn(xs[k], inc);
+            double dn = __dadd_rn(d, inc);
+            if (fz.periodic) xn = wrap(xn, pp.L[k]);
+            s.at(DX + k, i) = dn;
+            xs[k] = xn;
+            if (fz.track || fz.local) {
+                double e = dn - fz.bd[(size_t)k * N + i];
+                m = fma(e, e, m);
+                if (fz.local) l[k] = (float)(fz.bx[(size_t)k * N + i] + e);
+            }
+        }
+        s.at(VX + k, i) = v;
+    }
+    if (fz.pos_next) {
+        fz.pos_next[i] = make_double4(xs[0], xs[1], xs[2], 0.0);
+        if (fz.local) fz.posl_next[i] = make_float4(l[0], l[1], l[2], 0.f);
+    }
+    return fz.track ? m : 0.0;
+}
+
+// Warp max of the fused displacement into the next step's rebuild criterion.
+__device__ __forceinline__ void fused_track(const Fuse& fz, double m) {
+    if (fz.pos_next && fz.track) {
+        m = warp_max(m);
+        if ((threadIdx.x & 31) == 0 && m > 0.0)
+            atomicMax(&fz.sc->max_disp2_next, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
 // One 32-byte position in a single 256-bit load (sm_100 ld.global.v4.f64;
 // positions are double4 in cudaMalloc'd arrays, so always 32-byte aligned).
 __device__ __forceinline__ double4 ld_pos(const double4* p) {
@@ -508,9 +568,10 @@ __device__ __forceinline__ void pair_fp64(const PairParams& pp, double r2, doubl
 template <int KIND, bool SMALL, bool KICK, int BS = kThreads>
 static __global__ void __launch_bounds__(BS, 512 / BS)
 force_fp64_kernel(int N, const double4* __restrict__ pos, Soa s, const uint4* __restrict__ nbr4,
-                  const int* __restrict__ cnt, PairParams pp, double* __restrict__ partials) {
+                  const int* __restrict__ cnt, PairParams pp, double* __restrict__ partials, Fuse fu) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double acc[4] = {0, 0, 0, 0};  // sum v^2, sum pe_i, sum w_i, sum d^2
+    double m = 0.0;
     if (i < N) {
         const double4 xi = pos[i];
         bool near = !(xi.x >= pp.near_lo && xi.x < pp.near_hi[0] && xi.y >= pp.near_lo &&
@@ -550,17 +611,11 @@ force_fp64_kernel(int N, const double4* __restrict__ pos, Soa s, const uint4* __
         acc[1] = pe;
         acc[2] = w;
         if (KICK) {
-            double f3[3] = {fx, fy, fz};
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                double v = kick(s.at(VX + k, i), f3[k], pp.dt);
-                s.at(VX + k, i) = v;
-                acc[0] = fma(v, v, acc[0]);
-                double d = s.at(DX + k, i);
-                acc[3] = fma(d, d, acc[3]);
-            }
+            const double f3[3] = {fx, fy, fz};
+            m = step_epilogue(N, i, s, xi, f3, pp, fu, acc);
         }
     }
+    if (KICK) fused_track(fu, m);
     block_sum<4, BS>(acc);
     if (threadIdx.x == 0)
         for (int q = 0; q < 4; ++q) partials[(size_t)blockIdx.x * 4 + q] = acc[q];
@@ -608,7 +663,9 @@ finalize_kernel(const double* __restrict__ partials, int nblocks, int N, double 
             sc->nonfinite = 1;
         }
         if (mode != 2) {  // a measurement changes nothing that a rebuild depends on
-            sc->max_disp2 = 0ull;
+            // the next step's displacement (a fused epilogue's, else 0 for kick_drift)
+            sc->max_disp2 = sc->max_disp2_next;
+            sc->max_disp2_next = 0ull;
             sc->need_rebuild = 0;
         }
     }

@@ -84,9 +84,10 @@ template <bool KICK, int BS = kThreads>
 static __global__ void __launch_bounds__(BS, 512 / BS)
 force_mixed_kernel(int N, const float4* __restrict__ posl, Soa s, const uint4* __restrict__ nbr4,
                    const int* __restrict__ cnt, PairParams pp, MixedParams mp,
-                   double* __restrict__ partials) {
+                   double* __restrict__ partials, Fuse fu) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double acc[4] = {0, 0, 0, 0};
+    double m = 0.0;
     const float2 na_xy = make_float2(-mp.a[0], -mp.a[1]);
     const float az = mp.a[2];
     const float2 unbias = make_float2(-8388609.0f, -8388609.0f);
@@ -150,17 +151,12 @@ force_mixed_kernel(int N, const float4* __restrict__ posl, Soa s, const uint4* _
         acc[1] = pe;
         acc[2] = w;
         if (KICK) {
-            double f3[3] = {fx, fy, fz};
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                double v = kick(s.at(VX + k, i), f3[k], pp.dt);
-                s.at(VX + k, i) = v;
-                acc[0] = fma(v, v, acc[0]);
-                double d = s.at(DX + k, i);
-                acc[3] = fma(d, d, acc[3]);
-            }
+            const double f3[3] = {fx, fy, fz};
+            const double4 x = fu.pos_next ? fu.pos[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+            m = step_epilogue(N, i, s, x, f3, pp, fu, acc);
         }
     }
+    if (KICK) fused_track(fu, m);
     block_sum<4, BS>(acc);
     if (threadIdx.x == 0)
         for (int q = 0; q < 4; ++q) partials[(size_t)blockIdx.x * 4 + q] = acc[q];
