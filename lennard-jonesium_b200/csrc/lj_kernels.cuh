@@ -322,14 +322,16 @@ build_list_kernel(int N, const double4* __restrict__ pos, const float4* __restri
 
 // Warp-per-cell list build for grids of >= 3 cells per axis (the minimum-image
 // form).  One warp owns one list cell: lanes hold the cell's atoms (in chunks of
-// 32).  For each of the 27 stencil cells the warp stages 32 candidates at a
-// time in shared memory (one coalesced load, stored negated and as separate
-// x / y / z rows), and every lane tests every staged candidate through
-// broadcast reads, two candidates per instruction with Blackwell's packed
-// FP32x2 add / multiply / fma.  The test loop only sets bits of a hit mask; a
-// short per-lane loop over the set bits then appends the entries, so the
-// append code is not issued once per candidate.  Each lane collects entries in
-// a 4-entry shared buffer and writes whole groups (one 16-byte store).
+// 32).  Atoms are stored cell by cell with z fastest, so the three stencil
+// cells z - 1, z, z + 1 of each of the 9 stencil columns are one contiguous
+// slot range (two where the column wraps in z).  The warp walks each range in
+// chunks of 32 candidates staged in shared memory (one coalesced load, stored
+// negated as separate x / y / z rows); every lane tests the staged candidates
+// through broadcast reads, two per instruction with Blackwell's packed FP32x2
+// add / multiply / fma, in unrolled blocks of 8 that only set bits of a hit
+// mask.  A short per-lane loop over the set bits then appends the entries, so
+// the append code is not issued once per candidate.  Each lane collects entries
+// in a 4-entry shared buffer and writes whole groups (one 16-byte store).
 // Entries, their order (stencil cell, then slot) and the candidate radius are
 // those of build_list_kernel<false>.
 constexpr int kBuildWarps = 4;
@@ -357,6 +359,15 @@ build_list_warp_kernel(int N, const double4* __restrict__ pos, const float4* __r
     unsigned (&grp)[4] = grp_s[warp][lane];
     if (c < ncell) {
         int ca = c / (g.n[1] * g.n[2]), cb = (c / g.n[2]) % g.n[1], cc = c % g.n[2];
+        int nz = g.n[2];
+        // the column's z cells d = -1, 0, 1 as at most two contiguous pieces,
+        // split where the column wraps (each piece has one z image)
+        int npc = 1, pd0[2] = {-1, 0}, pd1[2] = {1, 1}, pic[2] = {0, 0};
+        if (cc == 0) {
+            npc = 2; pd0[0] = -1; pd1[0] = -1; pic[0] = -1; pd0[1] = 0; pd1[1] = 1; pic[1] = 0;
+        } else if (cc == nz - 1) {
+            npc = 2; pd0[0] = -1; pd1[0] = 0; pic[0] = 0; pd0[1] = 1; pd1[1] = 1; pic[1] = 1;
+        }
         int hs = start[c], he = start[c + 1];
         for (int h0 = hs; h0 < he; h0 += 32) {
             int i = h0 + lane;
@@ -369,16 +380,17 @@ build_list_warp_kernel(int N, const double4* __restrict__ pos, const float4* __r
                 for (int b = -1; b <= 1; ++b) {
                     int nb = cb + b, ib = nb < 0 ? -1 : (nb >= g.n[1] ? 1 : 0);
                     nb -= ib * g.n[1];
-                    for (int d = -1; d <= 1; ++d) {
-                        int nc = cc + d, ic = nc < 0 ? -1 : (nc >= g.n[2] ? 1 : 0);
-                        nc -= ic * g.n[2];
-                        int cell = g.flat(na, nb, nc);
-                        // home atom shifted by the lattice image of this stencil cell
-                        float2 sx = make_float2(xi.x - ia * Lf.x, xi.x - ia * Lf.x);
-                        float2 sy = make_float2(xi.y - ib * Lf.y, xi.y - ib * Lf.y);
-                        float2 sz = make_float2(xi.z - ic * Lf.z, xi.z - ic * Lf.z);
-                        unsigned code = offset_code(a, b, d);
-                        int js = start[cell], je = start[cell + 1];
+                    int col = g.flat(na, nb, 0);
+                    // slot where the d = 0 and d = 1 cells of this column begin
+                    int s0 = start[col + cc], s1 = start[col + (cc + 1 == nz ? 0 : cc + 1)];
+                    float2 sx = make_float2(xi.x - ia * Lf.x, xi.x - ia * Lf.x);
+                    float2 sy = make_float2(xi.y - ib * Lf.y, xi.y - ib * Lf.y);
+                    for (int pc = 0; pc < npc; ++pc) {
+                        int zlo = cc + pd0[pc], zhi = cc + pd1[pc];
+                        zlo += zlo < 0 ? nz : (zlo >= nz ? -nz : 0);
+                        zhi += zhi < 0 ? nz : (zhi >= nz ? -nz : 0);
+                        int js = start[col + zlo], je = start[col + zhi + 1];
+                        float2 sz = make_float2(xi.z - pic[pc] * Lf.z, xi.z - pic[pc] * Lf.z);
                         for (int j0 = js; j0 < je; j0 += 32) {
                             int cntj = min(32, je - j0);
                             __syncwarp();
@@ -388,23 +400,33 @@ build_list_warp_kernel(int N, const double4* __restrict__ pos, const float4* __r
                             cxs[warp][2][lane] = -q.z;
                             __syncwarp();
                             unsigned mask = 0;
-                            for (int t = 0; t < cntj; t += 2) {
-                                float2 qx = *reinterpret_cast<const float2*>(&cxs[warp][0][t]);
-                                float2 qy = *reinterpret_cast<const float2*>(&cxs[warp][1][t]);
-                                float2 qz = *reinterpret_cast<const float2*>(&cxs[warp][2][t]);
-                                float2 dx = __fadd2_rn(sx, qx), dy = __fadd2_rn(sy, qy), dz = __fadd2_rn(sz, qz);
-                                float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-                                mask |= (r2.x < cut2 ? 1u : 0u) << t;
-                                mask |= (r2.y < cut2 ? 2u : 0u) << t;
+                            for (int t0 = 0; t0 < cntj; t0 += 8) {
+                                unsigned sub = 0;
+#pragma unroll
+                                for (int t = 0; t < 8; t += 2) {
+                                    float2 qx = *reinterpret_cast<const float2*>(&cxs[warp][0][t0 + t]);
+                                    float2 qy = *reinterpret_cast<const float2*>(&cxs[warp][1][t0 + t]);
+                                    float2 qz = *reinterpret_cast<const float2*>(&cxs[warp][2][t0 + t]);
+                                    float2 dx = __fadd2_rn(sx, qx), dy = __fadd2_rn(sy, qy), dz = __fadd2_rn(sz, qz);
+                                    float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+                                    sub |= (r2.x < cut2 ? 1u : 0u) << t;
+                                    sub |= (r2.y < cut2 ? 2u : 0u) << t;
+                                }
+                                mask |= sub << t0;
                             }
-                            if (cntj < 32) mask &= (1u << cntj) - 1u;  // the odd tail reads a far-away filler
+                            if (cntj < 32) mask &= (1u << cntj) - 1u;  // fillers past the range
                             unsigned self = (unsigned)(i - j0);
                             if (self < 32u) mask &= ~(1u << self);
                             if (!own) mask = 0;
                             while (mask) {
                                 int t = __ffs(mask) - 1;
                                 mask &= mask - 1;
-                                append_entry(grp, n, cap, make_entry((unsigned)(j0 + t), code), nbr4, N, i);
+                                int j = j0 + t;
+                                // this piece's z offset of slot j: the cell it lies in
+                                int d = pd0[pc];
+                                if (d < 0 && pd1[pc] >= 0 && j >= s0) d = 0;
+                                if (d < 1 && pd1[pc] >= 1 && j >= s1) d = 1;
+                                append_entry(grp, n, cap, make_entry((unsigned)j, offset_code(a, b, d)), nbr4, N, i);
                             }
                         }
                     }
