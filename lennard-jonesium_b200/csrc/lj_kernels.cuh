@@ -368,6 +368,7 @@ build_list_warp_kernel(int N, const double4* __restrict__ pos, const float4* __r
         } else if (cc == nz - 1) {
             npc = 2; pd0[0] = -1; pd1[0] = 0; pic[0] = 0; pd0[1] = 1; pd1[1] = 1; pic[1] = 1;
         }
+        const float2 mcut2 = make_float2(-cut2, -cut2);
         int hs = start[c], he = start[c + 1];
         for (int h0 = hs; h0 < he; h0 += 32) {
             int i = h0 + lane;
@@ -401,18 +402,27 @@ build_list_warp_kernel(int N, const double4* __restrict__ pos, const float4* __r
                             __syncwarp();
                             unsigned mask = 0;
                             for (int t0 = 0; t0 < cntj; t0 += 8) {
+                                // r2 < cut2 exactly when r2 - cut2 is negative: its sign bit
+                                // is shifted into `sub`, first candidate highest
                                 unsigned sub = 0;
 #pragma unroll
-                                for (int t = 0; t < 8; t += 2) {
-                                    float2 qx = *reinterpret_cast<const float2*>(&cxs[warp][0][t0 + t]);
-                                    float2 qy = *reinterpret_cast<const float2*>(&cxs[warp][1][t0 + t]);
-                                    float2 qz = *reinterpret_cast<const float2*>(&cxs[warp][2][t0 + t]);
-                                    float2 dx = __fadd2_rn(sx, qx), dy = __fadd2_rn(sy, qy), dz = __fadd2_rn(sz, qz);
-                                    float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-                                    sub |= (r2.x < cut2 ? 1u : 0u) << t;
-                                    sub |= (r2.y < cut2 ? 2u : 0u) << t;
+                                for (int t = 0; t < 8; t += 4) {
+                                    float4 qx = *reinterpret_cast<const float4*>(&cxs[warp][0][t0 + t]);
+                                    float4 qy = *reinterpret_cast<const float4*>(&cxs[warp][1][t0 + t]);
+                                    float4 qz = *reinterpret_cast<const float4*>(&cxs[warp][2][t0 + t]);
+#pragma unroll
+                                    for (int h = 0; h < 2; ++h) {
+                                        float2 px = h ? make_float2(qx.z, qx.w) : make_float2(qx.x, qx.y);
+                                        float2 py = h ? make_float2(qy.z, qy.w) : make_float2(qy.x, qy.y);
+                                        float2 pz = h ? make_float2(qz.z, qz.w) : make_float2(qz.x, qz.y);
+                                        float2 dx = __fadd2_rn(sx, px), dy = __fadd2_rn(sy, py), dz = __fadd2_rn(sz, pz);
+                                        float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+                                        float2 sg = __fadd2_rn(r2, mcut2);
+                                        sub = __funnelshift_l(__float_as_uint(sg.x), sub, 1);
+                                        sub = __funnelshift_l(__float_as_uint(sg.y), sub, 1);
+                                    }
                                 }
-                                mask |= sub << t0;
+                                mask |= __brev(sub) >> (24 - t0);
                             }
                             if (cntj < 32) mask &= (1u << cntj) - 1u;  // fillers past the range
                             unsigned self = (unsigned)(i - j0);
