@@ -270,7 +270,7 @@ def run_ours(args, ws, rank, local):
                                     device=local)
             tuning[prec] = dict(kw, tuned_ms_per_step=tuned_ms)
         else:
-            kw = {}
+            kw = {"skin": args.skin, "force_block": args.block}
         g = GpuSystem(N_ATOMS, L, cutoff=WORK["rc"], dt=WORK["dt"], precision=prec, device=local, **kw)
         g.upload(x, v=v)
         g.step_async(args.warmup)
@@ -435,6 +435,118 @@ def run_sweep_bench(args):
     print(json.dumps(line), flush=True)
 
 
+LONG = dict(n_cells=100, T=0.9, rho=0.8, rc=2.5, dt=0.004, seed=2718, rdf_every=100, rdf_bins=200, rdf_rmax=4.0)
+
+
+def run_long_bench(args):
+    """4M-atom (4 * 100^3 FCC) run at rho = 0.8, T = 0.9, dt = 0.004: the mixed path
+    with an RDF histogram (200 bins to 4 sigma) every 100 steps, and the same run on
+    the FP64 path for the drift comparison.  Device time of both runs (steps and RDF
+    sampling) by CUDA events on each engine's stream."""
+    import numpy as np
+    import torch
+    from lennardjonesium import GpuSystem, initial_condition
+    N = 4 * LONG["n_cells"] ** 3
+    x, v, L = initial_condition(N, LONG["T"], LONG["rho"], LONG["seed"])
+    steps = max(LONG["rdf_every"], args.long_steps - args.long_steps % LONG["rdf_every"])
+    out = {}
+    for prec in ("mixed", "fp64"):
+        with GpuSystem(N, L, cutoff=LONG["rc"], dt=LONG["dt"], precision=prec) as g:
+            g.upload(x, v=v)
+            g.step(8)  # graph capture and first neighbour list outside the timed region
+            g.upload(x, v=v)
+            te = []
+            hist = np.zeros(LONG["rdf_bins"])
+            stream = torch.cuda.ExternalStream(g.stream)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(steps // LONG["rdf_every"]):
+                te.append(g.step(LONG["rdf_every"])[:, 3])
+                hist += g.rdf(LONG["rdf_bins"], LONG["rdf_rmax"])
+            e1.record(stream)
+            e1.synchronize()
+            sec = e0.elapsed_time(e1) / 1e3
+            te = np.concatenate(te)
+            w = 200
+            out[prec] = {"ms_per_step": 1e3 * sec / steps, "atom_steps_per_s": N * steps / sec,
+                         "abs_rel_drift": float(abs(te[-w:].mean() - te[:w].mean()) / abs(te[:w].mean())),
+                         "max_rel_excursion": float(abs(te - te[0]).max() / abs(te[0])),
+                         "list_builds": g.stats()["list_builds"], "hist": hist}
+    # normalised g(r) of both runs and their largest difference
+    edges = np.linspace(0.0, LONG["rdf_rmax"], LONG["rdf_bins"] + 1)
+    shell = 4.0 / 3.0 * np.pi * (edges[1:] ** 3 - edges[:-1] ** 3)
+    samples = steps // LONG["rdf_every"]
+    # ordered pairs: g(r) = hist / (samples N rho shell volume)
+    gr = {p: out[p].pop("hist") / (samples * N * (N / L ** 3) * shell) for p in out}
+    peak = int(np.argmax(gr["mixed"]))
+    line = {"metric": "4M-atom mixed-precision NVE with RDF sampling (atom-steps/s, incl. sampling)",
+            "unit": "atom-steps/s", "value": out["mixed"]["atom_steps_per_s"], "steps": steps, "atoms": N,
+            "mixed": out["mixed"], "fp64": out["fp64"],
+            "speedup_vs_fp64": out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"],
+            "rdf": {"samples": samples, "bins": LONG["rdf_bins"], "rmax": LONG["rdf_rmax"],
+                    "first_peak_r": float(0.5 * (edges[peak] + edges[peak + 1])),
+                    "first_peak_g": float(gr["mixed"][peak]),
+                    "max_abs_diff_vs_fp64": float(np.abs(gr["mixed"] - gr["fp64"]).max())},
+            "config": {"workload": f"FCC LJ fluid N={N} (4*100^3), rho=0.8, T=0.9, rc=2.5, dt=0.004, seeded MB "
+                                   "velocities; RDF 200 bins to 4 sigma every 100 steps", "data": "synthetic"}}
+    print(json.dumps(line), flush=True)
+
+
+ADJ = dict(N=4000, rho=0.8, T=1.2, steps=200, k=20, dt=0.005, seed=4000, h=1e-6)
+
+
+def run_adjoint_bench(args):
+    """Differentiable NVE at N = 4000 (4 * 10^3 FCC), rho = 0.8, T = 1.2, 200 steps,
+    checkpoints every 20: time of one forward pass and of one backward (adjoint)
+    pass on the device, and the gradient against central finite differences
+    (h = 1e-6) for epsilon, sigma and a random unit direction of the positions."""
+    import numpy as np
+    import torch
+    from lennardjonesium import AdjointNVE, initial_condition
+    x, v, L = initial_condition(ADJ["N"], ADJ["T"], ADJ["rho"], ADJ["seed"])
+    x, v = x[:, :3].copy(), v[:, :3].copy()
+    with AdjointNVE(ADJ["N"], L, ADJ["steps"], checkpoint_every=ADJ["k"], time_delta=ADJ["dt"]) as e:
+        e.forward(x, v)
+        e.backward(1.0, 1.0)  # warm-up
+        torch.cuda.synchronize()
+        reps = max(3, min(args.steps, 20))
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            e.forward(x, v)
+        t1 = time.perf_counter()
+        for _ in range(reps):
+            g = e.backward(1.0, 1.0)
+        t2 = time.perf_counter()
+        pe, p, _ = e.forward(x, v)
+        g = e.backward(1.0, 1.0)
+        rng = np.random.default_rng(1)
+        d = rng.standard_normal(x.shape)
+        d /= np.linalg.norm(d)
+        h = ADJ["h"]
+
+        def loss(xs, eps, sig):
+            e.set_potential(eps, sig)
+            a, b, _ = e.forward(xs, v)
+            return a + b
+
+        checks = {"epsilon": ((loss(x, 1 + h, 1) - loss(x, 1 - h, 1)) / (2 * h), g["epsilon"]),
+                  "sigma": ((loss(x, 1, 1 + h) - loss(x, 1, 1 - h)) / (2 * h), g["sigma"]),
+                  "x0_direction": ((loss(x + h * d, 1, 1) - loss(x - h * d, 1, 1)) / (2 * h), float((g["x0"] * d).sum()))}
+    fwd, bwd = (t1 - t0) / reps, (t2 - t1) / reps
+    line = {"metric": "differentiable NVE gradient (forward + adjoint) per second", "unit": "gradients/s",
+            "value": 1.0 / (fwd + bwd), "forward_ms": 1e3 * fwd, "backward_ms": 1e3 * bwd,
+            "forward_atom_steps_per_s": ADJ["N"] * ADJ["steps"] / fwd,
+            "loss": {"pe_avg": pe, "p_avg": p},
+            "fd_check": {k: {"central_difference": fd, "adjoint": ad, "rel_err": abs(ad - fd) / abs(fd)}
+                         for k, (fd, ad) in checks.items()},
+            "config": {"workload": "N=4000 (4*10^3 FCC), rho=0.8, T=1.2, rc=2.5 sigma, dt=0.005, 200 steps, FP64, "
+                                   "checkpoint every 20; loss = time-averaged PE + virial pressure",
+                       "timing": "wall clock around synchronised calls (host-driven per-step launches)",
+                       "data": "synthetic"}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -445,8 +557,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="skip the autotuner (skin and pair-kernel block size per precision)")
-    ap.add_argument("--workload", choices=("single", "sweep"), default="single",
-                    help="single: the 1M-atom benchmark line; sweep: batched vs sequential 64-system sweep")
+    ap.add_argument("--skin", type=float, default=None, help="with --no-autotune: Verlet skin (default 0.3)")
+    ap.add_argument("--block", type=int, default=0, help="with --no-autotune: pair-kernel block size (default 128)")
+    ap.add_argument("--workload", choices=("single", "sweep", "long", "adjoint"), default="single",
+                    help="single: the 1M-atom benchmark line; sweep: batched vs sequential 64-system sweep; "
+                         "long: 4M-atom mixed-precision run with RDF sampling against FP64; "
+                         "adjoint: differentiable NVE gradient at N = 4000")
+    ap.add_argument("--long-steps", type=int, default=20000, help="steps of the long workload")
     ap.add_argument("--cells", type=int, default=64,
                     help="FCC cells per box edge (N = 4 cells^3); 64 is the benchmark workload")
     args = ap.parse_args()
@@ -457,6 +574,12 @@ def main():
         args.warmup = 3
     if args.workload == "sweep":
         run_sweep_bench(args)
+        return
+    if args.workload == "long":
+        run_long_bench(args)
+        return
+    if args.workload == "adjoint":
+        run_adjoint_bench(args)
         return
     if args.impl == "reference":
         # CPU only: rank 0 runs the reference arm, the other ranks exit at once

@@ -117,12 +117,15 @@ static __global__ void ad_sort_cells_kernel(int ncell, const int* __restrict__ s
 }
 
 // Exact neighbour list over the 27-cell stencil (minimum image): every j with
-// r_ij^2 < rc^2, in stencil-then-id order, stored [slot][atom].
-static __global__ void ad_list_kernel(int N, const double4* __restrict__ x, Grid g, const int* __restrict__ cell_of,
-                                      const int* __restrict__ start, const int* __restrict__ members, AdjParams P,
-                                      int* __restrict__ nbr, int* __restrict__ cnt, int* __restrict__ overflow) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
+// r_ij^2 < rc^2, in stencil-then-id order, stored [slot][atom].  One warp per
+// atom: the lanes test 32 candidates of a cell at a time and the hits are
+// compacted in candidate order (ballot + prefix count).
+static __global__ void __launch_bounds__(kThreads)
+ad_list_kernel(int N, const double4* __restrict__ x, Grid g, const int* __restrict__ cell_of,
+               const int* __restrict__ start, const int* __restrict__ members, AdjParams P,
+               int* __restrict__ nbr, int* __restrict__ cnt, int* __restrict__ overflow) {
+    int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (i >= N) return;  // uniform across the warp
     double4 xi = x[i];
     int c = cell_of[i];
     int ca = c / (g.n[1] * g.n[2]), cb = (c / g.n[2]) % g.n[1], cc = c % g.n[2];
@@ -131,21 +134,32 @@ static __global__ void ad_list_kernel(int N, const double4* __restrict__ x, Grid
         for (int b = -1; b <= 1; ++b)
             for (int d = -1; d <= 1; ++d) {
                 int cell = g.flat((ca + a + g.n[0]) % g.n[0], (cb + b + g.n[1]) % g.n[1], (cc + d + g.n[2]) % g.n[2]);
-                for (int k = start[cell]; k < start[cell + 1]; ++k) {
-                    int j = members[k];
-                    if (j == i) continue;
-                    double4 xj = x[j];
-                    double dx = mimg(xi.x - xj.x, P.L[0], P.halfL[0]);
-                    double dy = mimg(xi.y - xj.y, P.L[1], P.halfL[1]);
-                    double dz = mimg(xi.z - xj.z, P.L[2], P.halfL[2]);
-                    if (dx * dx + dy * dy + dz * dz < P.rc2) {
-                        if (n < kAdjCap) nbr[(size_t)n * N + i] = j;
-                        ++n;
+                int ke = start[cell + 1];
+                for (int k0 = start[cell]; k0 < ke; k0 += 32) {
+                    int k = k0 + lane, j = -1;
+                    bool hit = false;
+                    if (k < ke) {
+                        j = members[k];
+                        if (j != i) {
+                            double4 xj = x[j];
+                            double dx = mimg(xi.x - xj.x, P.L[0], P.halfL[0]);
+                            double dy = mimg(xi.y - xj.y, P.L[1], P.halfL[1]);
+                            double dz = mimg(xi.z - xj.z, P.L[2], P.halfL[2]);
+                            hit = dx * dx + dy * dy + dz * dz < P.rc2;
+                        }
                     }
+                    unsigned m = __ballot_sync(0xffffffffu, hit);
+                    if (hit) {
+                        int slot = n + __popc(m & ((1u << lane) - 1u));
+                        if (slot < kAdjCap) nbr[(size_t)slot * N + i] = j;
+                    }
+                    n += __popc(m);
                 }
             }
-    cnt[i] = min(n, kAdjCap);
-    if (n > kAdjCap) atomicExch(overflow, 1);
+    if (lane == 0) {
+        cnt[i] = min(n, kAdjCap);
+        if (n > kAdjCap) atomicExch(overflow, 1);
+    }
 }
 
 template <int Q>
@@ -355,8 +369,8 @@ int build_list(lj_adj_ctx* a) {
     scan_apply_kernel<false><<<ntiles, 1024, 0, a->stream>>>(a->count, nc, a->tiles, a->start, open);  // zeroes count
     ad_members_kernel<<<nb(N), kThreads, 0, a->stream>>>(N, a->cell_of, a->rank, a->start, a->members);
     ad_sort_cells_kernel<<<nb(nc), kThreads, 0, a->stream>>>(nc, a->start, a->members);
-    ad_list_kernel<<<nb(N), kThreads, 0, a->stream>>>(N, a->x, a->g, a->cell_of, a->start, a->members, a->P, a->nbr,
-                                                      a->cnt, a->overflow);
+    ad_list_kernel<<<nb(32 * N), kThreads, 0, a->stream>>>(N, a->x, a->g, a->cell_of, a->start, a->members, a->P,
+                                                           a->nbr, a->cnt, a->overflow);
     AK(cudaGetLastError());
     return LJ_OK;
 }
@@ -408,7 +422,7 @@ extern "C" {
 int lj_adj_create(const lj_adj_params* p, lj_adj_ctx** out) {
     if (!out) return LJ_ERR_ARG;
     *out = nullptr;
-    if (!p || p->particle_count < 2 || p->steps < 1 || p->checkpoint_every < 1 || !(p->time_delta > 0) ||
+    if (!p || p->particle_count < 2 || p->particle_count > (1 << 25) || p->steps < 1 || p->checkpoint_every < 1 || !(p->time_delta > 0) ||
         !(p->cutoff_sigma * p->cutoff_sigma > std::cbrt(2.0)) || !std::isfinite(p->cutoff_sigma))
         return LJ_ERR_ARG;  // lennard_jones_force.cpp:45 asserts rc^2 > 2^(1/3)
     for (int k = 0; k < 3; ++k)

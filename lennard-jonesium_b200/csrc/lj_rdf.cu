@@ -6,8 +6,9 @@
 // dd > L/2, fma-ordered r^2, IEEE sqrt), so histograms agree bit-for-bit.
 //
 // Boxes with at least 3 cells of edge >= rmax per axis use a cell list over
-// the 27-cell stencil (counting sort into an RDF grid, positions copied in that
-// order); smaller boxes use all pairs.  Each block accumulates a shared-memory
+// the half-shell stencil (counting sort into an RDF grid, positions copied in
+// that order; each unordered pair evaluated once and counted twice); smaller
+// boxes use all pairs.  Each block accumulates a shared-memory
 // histogram and adds it to the global 64-bit histogram once.
 
 #include <atomic>
@@ -25,6 +26,7 @@ __device__ __forceinline__ double min_image(double dd, double L, double halfL) {
     return __dsub_rn(dd, __dmul_rn(img, L));
 }
 
+template <unsigned INC>
 __device__ __forceinline__ void rdf_count(const double4& xi, const double4& xj, const PairParams& pp,
                                           double rmax2, double inv_dr, int nbins, unsigned* sh) {
     double sx = min_image(__dsub_rn(xi.x, xj.x), pp.L[0], pp.halfL[0]);
@@ -33,7 +35,7 @@ __device__ __forceinline__ void rdf_count(const double4& xi, const double4& xj, 
     double r2 = norm2(sx, sy, sz);
     if (r2 < rmax2) {
         int b = (int)__dmul_rn(__dsqrt_rn(r2), inv_dr);
-        if (b < nbins) atomicAdd(&sh[b], 1u);
+        if (b < nbins) atomicAdd(&sh[b], INC);
     }
 }
 
@@ -53,7 +55,7 @@ rdf_all_pairs_kernel(int N, const double4* __restrict__ pos, PairParams pp, doub
     if (i < N) {
         double4 xi = pos[i];
         for (int j = 0; j < N; ++j)
-            if (j != i) rdf_count(xi, pos[j], pp, rmax2, inv_dr, nbins, sh);
+            if (j != i) rdf_count<1u>(xi, pos[j], pp, rmax2, inv_dr, nbins, sh);
     }
     flush(sh, nbins, hist);
 }
@@ -69,17 +71,18 @@ rdf_cells_kernel(int N, const double4* __restrict__ sorted, Grid g, const int* _
         double4 xi = sorted[i];
         int ci[3] = {cell_coord(xi.x, g.ratio[0], g.n[0]), cell_coord(xi.y, g.ratio[1], g.n[1]),
                      cell_coord(xi.z, g.ratio[2], g.n[2])};
-        for (int a = -1; a <= 1; ++a) {
-            int na = (ci[0] + a + g.n[0]) % g.n[0];
-            for (int b = -1; b <= 1; ++b) {
-                int nb = (ci[1] + b + g.n[1]) % g.n[1];
-                for (int c = -1; c <= 1; ++c) {
-                    int nc = (ci[2] + c + g.n[2]) % g.n[2];
-                    int cell = g.flat(na, nb, nc);
-                    for (int j = start[cell]; j < start[cell + 1]; ++j)
-                        if (j != i) rdf_count(xi, sorted[j], pp, rmax2, inv_dr, nbins, sh);
-                }
-            }
+        // half shell: the own cell's later atoms and the 13 stencil cells after
+        // the own cell in (a, b, c) order; each unordered pair is met once and
+        // counts for both ordered pairs (the separation of (j, i) is exactly the
+        // negated one of (i, j), so both fall in the same bin)
+        for (int j = i + 1; j < start[g.flat(ci[0], ci[1], ci[2]) + 1]; ++j)
+            rdf_count<2u>(xi, sorted[j], pp, rmax2, inv_dr, nbins, sh);
+        for (int s = 14; s < 27; ++s) {
+            int a = s / 9 - 1, b = (s / 3) % 3 - 1, c = s % 3 - 1;
+            int cell = g.flat((ci[0] + a + g.n[0]) % g.n[0], (ci[1] + b + g.n[1]) % g.n[1],
+                              (ci[2] + c + g.n[2]) % g.n[2]);
+            for (int j = start[cell]; j < start[cell + 1]; ++j)
+                rdf_count<2u>(xi, sorted[j], pp, rmax2, inv_dr, nbins, sh);
         }
     }
     flush(sh, nbins, hist);
