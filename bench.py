@@ -332,7 +332,8 @@ def run_ours(args, ws, rank, local):
             "phases_ms_per_step": {k: ph[k] / ph["steps"] for k in ("kick_drift_ms", "rebuild_ms", "force_ms",
                                                                      "finalize_ms")},
             "list_builds_per_step": ph["rebuilds"] / ph["steps"],
-            "tuning": tuning or "defaults (skin 0.3, 128 atoms per block)",
+            "tuning": tuning or {"fixed": True, "skin": 0.3 if args.skin is None else args.skin,
+                                 "force_block": args.block or 128},
             "fma_peaks_tflops": {"fp64": f64.value, "fp32": f32.value}}
     if ws == 1 and rank == 0 and not args.no_cpu_baseline:
         sys.path.insert(0, str(ROOT / "oracle"))
