@@ -29,6 +29,9 @@ namespace ljb {
 struct MixedParams {
     float rc2, inv_rc2, alpha, beta;
     float a[3];  // list-cell edge per axis
+    // the spline terms as functions of r^2: V = 4u(u - 1) + bq r^2 + abq,
+    // W = u(48u - 24) + wq r^2 with u = r^-6 (lennard_jones_force.cpp:107-119)
+    float bq, abq, wq;
 };
 
 inline MixedParams mixed_params(const PairParams& pp, const Grid& g) {
@@ -38,6 +41,9 @@ inline MixedParams mixed_params(const PairParams& pp, const Grid& g) {
     m.alpha = (float)pp.alpha;
     m.beta = (float)pp.beta;
     for (int k = 0; k < 3; ++k) m.a[k] = (float)(pp.L[k] / g.n[k]);
+    m.bq = (float)(pp.beta * pp.inv_rc2);
+    m.abq = (float)(pp.alpha - pp.beta);
+    m.wq = (float)(-2.0 * pp.beta * pp.inv_rc2);
     return m;
 }
 
@@ -95,27 +101,26 @@ force_mixed_kernel(int N, const float4* __restrict__ posl, Soa s, const uint4* _
         const float4 xi = posl[i];
         const float2 xi_xy = make_float2(xi.x, xi.y);
         double fx = 0, fy = 0, fz = 0, pe = 0, w = 0;
-        // list indices stream from HBM: keep three groups of them in flight
-        // (the neighbour positions, mostly L1/L2 hits, are gathered per group)
+        // list indices stream from HBM: two groups in flight ahead of the two
+        // being evaluated (the neighbour positions, mostly L1/L2 hits, are
+        // gathered per group)
         int ng = (cnt[i] + 3) >> 2;
         const uint4* lp = nbr4 + i;
         const uint4 z4 = make_uint4(0u, 0u, 0u, 0u);
-        uint4 L0 = ng > 0 ? __ldcs(lp) : z4;
-        uint4 L1 = ng > 1 ? __ldcs(lp + (size_t)N) : z4;
-        uint4 L2 = ng > 2 ? __ldcs(lp + 2 * (size_t)N) : z4;
-        // chunks of 2 groups = 8 neighbours summed in FP32, then added in FP64
-        float cx = 0.f, cy = 0.f, cz = 0.f, cv = 0.f, cw = 0.f;
-        for (int g = 0; g < ng; ++g) {
-            uint4 L3 = g + 3 < ng ? __ldcs(lp + (size_t)(g + 3) * N) : z4;
+        uint4 A = ng > 0 ? __ldcs(lp) : z4;
+        uint4 B = ng > 1 ? __ldcs(lp + (size_t)N) : z4;
+        const float2 mone = make_float2(-1.f, -1.f);
+        // one group: 4 neighbours into the FP32 chunk sums
+        auto group = [&](const uint4 grp, float& cx, float& cy, float& cz, float& cv, float& cw) {
             float4 Q[4];
-            gather4(posl, L0, Q);
-            const unsigned e[4] = {L0.x, L0.y, L0.z, L0.w};
+            gather4(posl, grp, Q);
+            const unsigned e[4] = {grp.x, grp.y, grp.z, grp.w};
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 // s = (xl_i - xl_j) - offset * a, the offset product exact
                 float2 t_xy = __fadd2_rn(make_float2(code_bias(e[u]), code_bias(e[u] >> 2)), unbias);
                 float tz = code_bias(e[u] >> 4) - 8388609.0f;
-                float2 d_xy = __fadd2_rn(xi_xy, make_float2(-Q[u].x, -Q[u].y));
+                float2 d_xy = __ffma2_rn(make_float2(Q[u].x, Q[u].y), mone, xi_xy);  // xi - q, one rounding
                 d_xy = __ffma2_rn(t_xy, na_xy, d_xy);
                 float dx = d_xy.x, dy = d_xy.y;
                 float dz = fmaf(-tz, az, xi.z - Q[u].z);
@@ -123,9 +128,8 @@ force_mixed_kernel(int N, const float4* __restrict__ posl, Soa s, const uint4* _
                 bool hit = r2 < mp.rc2;
                 float ir2 = rcp_approx(r2);
                 float ir6 = ir2 * ir2 * ir2;
-                float x = r2 * mp.inv_rc2;
-                float V = fmaf(4.f * ir6, ir6 - 1.f, fmaf(mp.beta, x - 1.f, mp.alpha));
-                float W = fmaf(24.f * ir6, fmaf(2.f, ir6, -1.f), -2.f * mp.beta * x);
+                float V = fmaf(4.f * ir6, ir6 - 1.f, fmaf(mp.bq, r2, mp.abq));
+                float W = fmaf(ir6, fmaf(48.f, ir6, -24.f), mp.wq * r2);
                 float f = hit ? W * ir2 : 0.f;
                 cx = fmaf(f, dx, cx);
                 cy = fmaf(f, dy, cy);
@@ -133,17 +137,21 @@ force_mixed_kernel(int N, const float4* __restrict__ posl, Soa s, const uint4* _
                 cv += hit ? V : 0.f;
                 cw += hit ? W : 0.f;
             }
-            if ((g & 1) || g + 1 == ng) {
-                fx += (double)cx;
-                fy += (double)cy;
-                fz += (double)cz;
-                pe += (double)cv;
-                w += (double)cw;
-                cx = cy = cz = cv = cw = 0.f;
-            }
-            L0 = L1;
-            L1 = L2;
-            L2 = L3;
+        };
+        // chunks of 2 groups = 8 neighbours summed in FP32, then added in FP64
+        for (int g = 0; g < ng; g += 2) {
+            uint4 C = g + 2 < ng ? __ldcs(lp + (size_t)(g + 2) * N) : z4;
+            uint4 D = g + 3 < ng ? __ldcs(lp + (size_t)(g + 3) * N) : z4;
+            float cx = 0.f, cy = 0.f, cz = 0.f, cv = 0.f, cw = 0.f;
+            group(A, cx, cy, cz, cv, cw);
+            if (g + 1 < ng) group(B, cx, cy, cz, cv, cw);
+            fx += (double)cx;
+            fy += (double)cy;
+            fz += (double)cz;
+            pe += (double)cv;
+            w += (double)cw;
+            A = C;
+            B = D;
         }
         s.at(FX, i) = fx;
         s.at(FY, i) = fy;
