@@ -612,16 +612,15 @@ force_fp64_kernel(int N, const double4* __restrict__ pos, Soa s, const uint4* __
         bool near = !(xi.x >= pp.near_lo && xi.x < pp.near_hi[0] && xi.y >= pp.near_lo &&
                       xi.y < pp.near_hi[1] && xi.z >= pp.near_lo && xi.z < pp.near_hi[2]);
         double fx = 0, fy = 0, fz = 0, pe = 0, w = 0;
-        // list indices stream from HBM: keep three groups of them in flight
+        // list indices stream from HBM: two groups in flight ahead of the two
+        // being evaluated
         int ng = (cnt[i] + 3) >> 2;
         const uint4* lp = nbr4 + i;
         const uint4 z4 = make_uint4(0u, 0u, 0u, 0u);
-        uint4 L0 = ng > 0 ? __ldcs(lp) : z4;
-        uint4 L1 = ng > 1 ? __ldcs(lp + (size_t)N) : z4;
-        uint4 L2 = ng > 2 ? __ldcs(lp + 2 * (size_t)N) : z4;
-        for (int g = 0; g < ng; ++g) {
-            uint4 L3 = g + 3 < ng ? __ldcs(lp + (size_t)(g + 3) * N) : z4;
-            unsigned e[4] = {L0.x, L0.y, L0.z, L0.w};
+        uint4 A = ng > 0 ? __ldcs(lp) : z4;
+        uint4 B = ng > 1 ? __ldcs(lp + (size_t)N) : z4;
+        auto group = [&](const uint4 grp) {
+            const unsigned e[4] = {grp.x, grp.y, grp.z, grp.w};
             double4 q[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) q[u] = ld_pos(pos + entry_slot(e[u]));
@@ -636,9 +635,14 @@ force_fp64_kernel(int N, const double4* __restrict__ pos, Soa s, const uint4* __
                 pe += V;
                 w += W;
             }
-            L0 = L1;
-            L1 = L2;
-            L2 = L3;
+        };
+        for (int g = 0; g < ng; g += 2) {
+            uint4 C = g + 2 < ng ? __ldcs(lp + (size_t)(g + 2) * N) : z4;
+            uint4 D = g + 3 < ng ? __ldcs(lp + (size_t)(g + 3) * N) : z4;
+            group(A);
+            if (g + 1 < ng) group(B);
+            A = C;
+            B = D;
         }
         s.at(FX, i) = fx;
         s.at(FY, i) = fy;
