@@ -199,8 +199,9 @@ int lj_gpu_step_timed(lj_ctx* ctx, int nsteps, lj_phase_times* out);
 /* Project autotuner: times `steps` steps of the system described by base and
  * the state (x, v; N x stride doubles) for each candidate skin (the list-cell
  * edge rc + skin and the rebuild frequency) and pair-kernel block size (atoms
- * per block: 64, 128, 256), each in a fresh context from the same state, and
- * writes the fastest parameters to *best (and its ms per step). */
+ * per block: 64, 128, 256) -- on the mixed path also the shared-memory tile
+ * kernel at 3 or 6 cells per tile -- each in a fresh context from the same
+ * state, and writes the fastest parameters to *best (and its ms per step). */
 int lj_gpu_autotune(const lj_params* base, const double* x, const double* v, int stride, int steps,
                     lj_params* best, double* best_ms_per_step);
 
