@@ -82,9 +82,13 @@ __device__ __forceinline__ void gather4(const float4* __restrict__ posl, const u
     q[3] = posl[entry_slot(grp.w)];
 }
 
-// Stencil offset of one axis from its 2-bit code c = i + 1: the FP32 value
-// 2^23 + c (exact), so that subtracting 2^23 + 1 gives i in {-1, 0, 1} exactly.
-__device__ __forceinline__ float code_bias(unsigned bits) { return __uint_as_float(0x4b000000u | (bits & 3u)); }
+// Stencil offset of one axis from its 2-bit code c = i + 1 at bit position
+// 2k: 2^23 + (c << 2k) is exact in FP32, so subtracting 2^23 + (1 << 2k)
+// gives i * 4^k exactly (no shift needed to extract the field); the offset
+// i * a is then that value times a / 4^k, an exact product.
+__device__ __forceinline__ float code_bias(unsigned e, unsigned field_mask) {
+    return __uint_as_float(0x4b000000u | (e & field_mask));
+}
 
 template <bool KICK, int BS = kThreads>
 static __global__ void __launch_bounds__(BS, 512 / BS)
@@ -94,9 +98,9 @@ force_mixed_kernel(int N, const float4* __restrict__ posl, Soa s, const uint4* _
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double acc[4] = {0, 0, 0, 0};
     double m = 0.0;
-    const float2 na_xy = make_float2(-mp.a[0], -mp.a[1]);
-    const float az = mp.a[2];
-    const float2 unbias = make_float2(-8388609.0f, -8388609.0f);
+    const float2 na_xy = make_float2(-mp.a[0], -0.25f * mp.a[1]);
+    const float az16 = 0.0625f * mp.a[2];
+    const float2 unbias = make_float2(-8388609.0f, -8388612.0f);
     if (i < N) {
         const float4 xi = posl[i];
         const float2 xi_xy = make_float2(xi.x, xi.y);
@@ -118,12 +122,12 @@ force_mixed_kernel(int N, const float4* __restrict__ posl, Soa s, const uint4* _
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 // s = (xl_i - xl_j) - offset * a, the offset product exact
-                float2 t_xy = __fadd2_rn(make_float2(code_bias(e[u]), code_bias(e[u] >> 2)), unbias);
-                float tz = code_bias(e[u] >> 4) - 8388609.0f;
+                float2 t_xy = __fadd2_rn(make_float2(code_bias(e[u], 0x3u), code_bias(e[u], 0xcu)), unbias);
+                float tz = code_bias(e[u], 0x30u) - 8388624.0f;
                 float2 d_xy = __ffma2_rn(make_float2(Q[u].x, Q[u].y), mone, xi_xy);  // xi - q, one rounding
                 d_xy = __ffma2_rn(t_xy, na_xy, d_xy);
                 float dx = d_xy.x, dy = d_xy.y;
-                float dz = fmaf(-tz, az, xi.z - Q[u].z);
+                float dz = fmaf(-tz, az16, xi.z - Q[u].z);
                 float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
                 bool hit = r2 < mp.rc2;
                 float ir2 = rcp_approx(r2);
