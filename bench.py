@@ -369,6 +369,34 @@ def sweep_systems():
     return out
 
 
+def sweep_files_arm():
+    """The same 8 x 8 (T, rho) grid through the drop-in API: lennardjonesium.run_sweep
+    with the reference's control protocol (equilibration with temperature
+    rescales, then 10 observations 500 steps apart) writing every run's four
+    files, N = 4000 per run (the sweep configuration has one particle count).
+    Wall clock of the whole call."""
+    import tempfile
+    import lennardjonesium as lj
+    sc = lj.SweepConfiguration()
+    sc.system.temperature_start, sc.system.temperature_stop, sc.system.temperature_steps = 0.5, 2.0, 8
+    sc.system.density_start, sc.system.density_stop, sc.system.density_steps = 0.05, 1.0, 8
+    sc.system.particle_count = 4000
+    sc.equilibration.adjustment_interval, sc.equilibration.steady_state_time = 200, 2000
+    sc.equilibration.timeout = 10000
+    sc.observation.observation_interval, sc.observation.observation_count = 500, 10
+    with tempfile.TemporaryDirectory() as d:
+        t0 = time.perf_counter()
+        res = lj.run_sweep(pathlib.Path(d) / "sweep.ini", echo_status=False, random_seed=2024,
+                           sweep_config_object=sc, batched=True)
+        sec = time.perf_counter() - t0
+    runs = res.completed + res.equilibration_aborted + res.observation_aborted
+    steps = sum(r.event_data.total_time_steps for r in runs)
+    return {"value": 4000 * steps / sec, "unit": "atom-steps/s", "seconds": sec, "runs": len(runs),
+            "completed": len(res.completed), "total_steps": steps,
+            "config": "T 0.5..2.0 x rho 0.05..1.0 (8 x 8), N=4000, eq: rescale check every 200 steps, steady "
+                      "2000, timeout 10000; obs: 10 x 500 steps; four files per run"}
+
+
 def run_sweep_bench(args):
     """Batched engine vs the same 64 systems run one after another on the GPU: identical
     protocol in both arms (chunks of 200 steps; during the first 2000 steps a system
@@ -425,11 +453,13 @@ def run_sweep_bench(args):
     torch.cuda.synchronize()
     t_seq = time.perf_counter() - t0
     atoms = sum(sy["N"] for sy in systems)
+    files = sweep_files_arm()
     line = {"metric": "batched 64-system (T, rho) sweep vs sequential GPU runs", "unit": "atom-steps/s",
             "value": atoms * total_steps / t_batched, "sequential": atoms * total_steps / t_seq,
             "speedup": t_seq / t_batched, "seconds_batched": t_batched, "seconds_sequential": t_seq,
             "systems": nsys, "atoms": atoms, "steps": total_steps,
             "identical_final_records": bool(np.array_equal(final_batched, final_seq)),
+            "run_sweep_files": files,
             "config": {"workload": "8x8 grid rho in [0.05,1.0] x T in [0.5,2.0], N=4n^3, n~U{5..20} (seed 2024), "
                                    "rc=2.5, dt=0.005, 2000 equilibration + 5000 production steps, FP64",
                        "timing": "wall clock around synchronised device work (host decisions included)"}}

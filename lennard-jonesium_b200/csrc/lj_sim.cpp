@@ -18,9 +18,13 @@
 #include <charconv>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <deque>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/lj_gpu.h"
@@ -29,40 +33,145 @@ namespace {
 
 // fmt's "{}" for a double: the shortest digits that round-trip, fixed notation
 // when the decimal exponent is in [-4, 16), scientific ("1e-05") otherwise, no
-// trailing ".0" for whole numbers.
-std::string fmt_double(double v) {
-    if (std::isnan(v)) return "nan";
-    if (std::isinf(v)) return v < 0 ? "-inf" : "inf";
-    if (v == 0) return std::signbit(v) ? "-0" : "0";
-    char buf[64];
+// trailing ".0" for whole numbers.  Writes at most 32 bytes to out and returns
+// the length.
+int fmt_double_buf(double v, char* out) {
+    char* o = out;
+    if (std::isnan(v)) return (int)(std::memcpy(out, "nan", 3), 3);
+    if (std::isinf(v)) {
+        if (v < 0) *o++ = '-';
+        std::memcpy(o, "inf", 3);
+        return (int)(o - out) + 3;
+    }
+    if (v == 0) {
+        if (std::signbit(v)) *o++ = '-';
+        *o++ = '0';
+        return (int)(o - out);
+    }
+    char buf[40];
     auto r = std::to_chars(buf, buf + sizeof buf, v, std::chars_format::scientific);
-    std::string sci(buf, r.ptr);
-    size_t epos = sci.find('e');
-    std::string mant = sci.substr(0, epos);
-    int exp = std::stoi(sci.substr(epos + 1));
-    bool neg = mant[0] == '-';
-    if (neg) mant = mant.substr(1);
-    std::string digits;
-    for (char ch : mant)
-        if (ch != '.') digits += ch;
-    std::string out;
+    const char* p = buf;
+    if (*p == '-') {
+        *o++ = '-';
+        ++p;
+    }
+    char digits[24];
+    int nd = 0;
+    for (; p < r.ptr && *p != 'e'; ++p)
+        if (*p != '.') digits[nd++] = *p;
+    ++p;  // 'e'
+    bool eneg = *p == '-';
+    if (*p == '-' || *p == '+') ++p;
+    int exp = 0;
+    for (; p < r.ptr; ++p) exp = exp * 10 + (*p - '0');
+    if (eneg) exp = -exp;
     if (exp >= -4 && exp < 16) {
         if (exp < 0) {
-            out = "0." + std::string(-exp - 1, '0') + digits;
-        } else if ((int)digits.size() <= exp + 1) {
-            out = digits + std::string(exp + 1 - digits.size(), '0');
+            *o++ = '0';
+            *o++ = '.';
+            for (int k = 0; k < -exp - 1; ++k) *o++ = '0';
+            for (int k = 0; k < nd; ++k) *o++ = digits[k];
+        } else if (nd <= exp + 1) {
+            for (int k = 0; k < nd; ++k) *o++ = digits[k];
+            for (int k = nd; k < exp + 1; ++k) *o++ = '0';
         } else {
-            out = digits.substr(0, exp + 1) + "." + digits.substr(exp + 1);
+            for (int k = 0; k <= exp; ++k) *o++ = digits[k];
+            *o++ = '.';
+            for (int k = exp + 1; k < nd; ++k) *o++ = digits[k];
         }
     } else {
-        out = digits.substr(0, 1);
-        if (digits.size() > 1) out += "." + digits.substr(1);
-        char eb[16];
-        std::snprintf(eb, sizeof eb, "e%c%02d", exp < 0 ? '-' : '+', std::abs(exp));
-        out += eb;
+        *o++ = digits[0];
+        if (nd > 1) {
+            *o++ = '.';
+            for (int k = 1; k < nd; ++k) *o++ = digits[k];
+        }
+        *o++ = 'e';
+        *o++ = exp < 0 ? '-' : '+';
+        int a = exp < 0 ? -exp : exp;
+        if (a >= 100) *o++ = (char)('0' + a / 100);
+        *o++ = (char)('0' + (a / 10) % 10);
+        *o++ = (char)('0' + a % 10);
     }
-    return neg ? "-" + out : out;
+    return (int)(o - out);
 }
+
+std::string fmt_double(double v) {
+    char b[40];
+    return std::string(b, (size_t)fmt_double_buf(v, b));
+}
+
+// One thermodynamics.csv row (output/sinks.cpp:116-130) into out (>= 320 bytes).
+int thermo_line(int step, const lj_thermo& r, char* out) {
+    char* o = out;
+    o = std::to_chars(o, o + 16, step).ptr;
+    for (double x : {r.time, r.kinetic_energy, r.potential_energy, r.total_energy, r.virial, r.temperature,
+                     r.mean_square_displacement}) {
+        *o++ = ',';
+        o += fmt_double_buf(x, o);
+    }
+    *o++ = '\n';
+    return (int)(o - out);
+}
+
+// Writes thermodynamics rows on a background thread, in the order they were
+// queued, so that formatting the rows of one chunk of steps overlaps the GPU's
+// next chunk.  drain() returns once every queued row is written.
+class ThermoWriter {
+  public:
+    struct Row {
+        FILE* f;
+        int step;
+        lj_thermo r;
+    };
+    ThermoWriter() : th_([this] { run(); }) {}
+    ~ThermoWriter() {
+        {
+            std::lock_guard<std::mutex> g(m_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        th_.join();
+    }
+    void push(std::vector<Row>&& rows) {
+        if (rows.empty()) return;
+        {
+            std::lock_guard<std::mutex> g(m_);
+            q_.push_back(std::move(rows));
+        }
+        cv_.notify_all();
+    }
+    void drain() {
+        std::unique_lock<std::mutex> g(m_);
+        idle_cv_.wait(g, [this] { return q_.empty() && !busy_; });
+    }
+
+  private:
+    void run() {
+        char line[320];
+        for (;;) {
+            std::vector<Row> job;
+            {
+                std::unique_lock<std::mutex> g(m_);
+                cv_.wait(g, [this] { return stop_ || !q_.empty(); });
+                if (q_.empty()) return;  // stop requested and nothing left
+                job = std::move(q_.front());
+                q_.pop_front();
+                busy_ = true;
+            }
+            for (const Row& row : job) std::fwrite(line, 1, (size_t)thermo_line(row.step, row.r, line), row.f);
+            {
+                std::lock_guard<std::mutex> g(m_);
+                busy_ = false;
+            }
+            idle_cv_.notify_all();
+        }
+    }
+    std::mutex m_;
+    std::condition_variable cv_, idle_cv_;
+    std::deque<std::vector<Row>> q_;
+    bool stop_ = false, busy_ = false;
+    std::thread th_;
+};
 
 // fmt's "{:.4g}"
 std::string fmt_g4(double v) {
@@ -120,12 +229,14 @@ struct Sinks {
             std::fflush(stdout);
         }
     }
+    std::vector<ThermoWriter::Row>* pending = nullptr;  // rows for a ThermoWriter, if one is attached
     void thermo_row(int step, const lj_thermo& r) {
-        std::string s = std::to_string(step) + "," + fmt_double(r.time) + "," + fmt_double(r.kinetic_energy) + "," +
-                        fmt_double(r.potential_energy) + "," + fmt_double(r.total_energy) + "," +
-                        fmt_double(r.virial) + "," + fmt_double(r.temperature) + "," +
-                        fmt_double(r.mean_square_displacement) + "\n";
-        std::fputs(s.c_str(), thermo);
+        if (pending) {
+            pending->push_back({thermo, step, r});
+            return;
+        }
+        char line[320];
+        std::fwrite(line, 1, (size_t)thermo_line(step, r, line), thermo);
     }
     void obs_row(int step, const Observation& o) {
         std::string s = std::to_string(step) + "," + fmt_double(o.temperature) + "," + fmt_double(o.density) + "," +
@@ -362,13 +473,19 @@ int lj_sim_run(const lj_sim_config* cfg, int echo, lj_sim_result* result) {
         return rc;
     }
     std::vector<lj_thermo> recs;
+    ThermoWriter writer;
+    std::vector<ThermoWriter::Row> rows;
+    ctl.out.pending = &rows;
     while (!ctl.finished() && rc == LJ_OK) {
         int K = std::max(1, ctl.next_decision() - ctl.time_step);
         recs.resize((size_t)K);
         if ((rc = lj_gpu_step(ctx, K, recs.data()))) break;
         for (int k = 0; k < K && !ctl.finished(); ++k)
             if (ctl.feed(recs[(size_t)k]) && (rc = lj_gpu_set_temperature(ctx, cfg->temperature, nullptr))) break;
+        writer.push(std::move(rows));  // formatted while the GPU runs the next chunk
+        rows.clear();
     }
+    writer.drain();
     if (rc == LJ_OK) {
         std::vector<double> F(4 * (size_t)N);
         rc = lj_gpu_download_state(ctx, x.data(), v.data(), nullptr, F.data(), 4, nullptr, nullptr, nullptr);
@@ -421,6 +538,9 @@ int lj_sim_run_batch(const lj_sim_config* cfgs, int n, int echo, lj_sim_result* 
         if (rc == LJ_OK) rc = ctl[(size_t)s].open(echo);
     }
     std::vector<lj_thermo> recs;
+    ThermoWriter writer;
+    std::vector<ThermoWriter::Row> rows;
+    for (auto& c : ctl) c.out.pending = &rows;
     int running = n;
     while (running > 0 && rc == LJ_OK) {
         int K = 1 << 30;
@@ -437,6 +557,9 @@ int lj_sim_run_batch(const lj_sim_config* cfgs, int n, int echo, lj_sim_result* 
             // a rescale precedes an abort on the same step, as in the reference's command queue
             if (rescale) rc = lj_batch_set_temperature(b, s, cfgs[s].temperature, nullptr);
             if (rc == LJ_OK && c.finished()) {
+                writer.push(std::move(rows));  // this run's rows before its snapshot
+                rows.clear();
+                writer.drain();
                 const int N = cfgs[s].particle_count;
                 std::vector<double> F(4 * (size_t)N);
                 rc = lj_batch_download_system(b, s, xs[(size_t)s].data(), vs[(size_t)s].data(), F.data(), 4);
@@ -445,7 +568,10 @@ int lj_sim_run_batch(const lj_sim_config* cfgs, int n, int echo, lj_sim_result* 
                 --running;
             }
         }
+        writer.push(std::move(rows));  // formatted while the GPU runs the next chunk
+        rows.clear();
     }
+    writer.drain();
     double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     for (int s = 0; s < n; ++s) {
         ctl[(size_t)s].out.close();
