@@ -669,10 +669,27 @@ force_fp64_kernel(int N, const double4* __restrict__ pos, Soa s, const uint4* __
 static __global__ void __launch_bounds__(1024)
 finalize_kernel(const double* __restrict__ partials, int nblocks, int N, double dt, int mode,
                 int forces_valid, Scalars* sc, double* __restrict__ ring, int ring_cap) {
+    // each thread sums blocks tid, tid + 1024, ... in that order; eight blocks'
+    // partials (32-byte loads) are in flight at a time
     double acc[4] = {0, 0, 0, 0};
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+    const double4* p4 = reinterpret_cast<const double4*>(partials);
+    for (int b0 = threadIdx.x; b0 < nblocks; b0 += 8 * 1024) {
+        double4 t[8];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) acc[q] += partials[(size_t)b * 4 + q];
+        for (int u = 0; u < 8; ++u) {
+            int b = b0 + u * 1024;
+            t[u] = b < nblocks ? p4[b] : make_double4(0.0, 0.0, 0.0, 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            if (b0 + u * 1024 < nblocks) {
+                acc[0] += t[u].x;
+                acc[1] += t[u].y;
+                acc[2] += t[u].z;
+                acc[3] += t[u].w;
+            }
+        }
+    }
     block_sum<4, 1024>(acc);
     if (threadIdx.x == 0) {
         if (forces_valid) {
