@@ -35,7 +35,7 @@ def _rank(rank, ws, port, out):
 
 def test_two_gloo_ranks():
     ws, port = 2, 29517
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_rank, args=(ws, port, out), nprocs=ws, join=True)
         res = dict(out)
