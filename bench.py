@@ -362,7 +362,7 @@ SWEEP = dict(systems=64, T=(0.5, 2.0, 8), rho=(0.05, 1.0, 8), n=(5, 20), rc=2.5,
 
 
 def sweep_systems():
-    """an 8 x 8 grid of rho in [0.05, 1.0] and T in [0.5, 2.0]
+    """The sweep workload: an 8 x 8 grid of rho in [0.05, 1.0] and T in [0.5, 2.0]
     (the reference's linspace, T outer), N = 4 n^3 with n ~ U{5..20} from a fixed seed."""
     import numpy as np
     from lennardjonesium import initial_condition

@@ -215,7 +215,7 @@ def test_seeded_run_matches_reference_rows(golden):
 
 
 def test_trajectory_vs_oracle():
-    """cfg 1 (N=864): 100 steps; chaos amplifies only summation-order rounding."""
+    """N = 864 (4*6^3, rho 0.8442, T 0.722): 100 steps; chaos amplifies only summation-order rounding."""
     x, v, L = ljref.initial_state(864, 0.722, 0.8442, 5489)
     ref = ljref.State(x, v=v)
     rth = ljref.run_steps(ref, L, 0.005, 100)
@@ -231,7 +231,7 @@ def test_trajectory_vs_oracle():
 
 
 def test_energy_conservation_fp64():
-    """cfg 1 for 2000 steps.  Melting from the FCC lattice raises TE by ~1e-3 in the
+    """N = 864 for 2000 steps.  Melting from the FCC lattice raises TE by ~1e-3 in the
     first ~200 steps in the reference algorithm too (the oracle shows the same
     transient); after it, TE is flat and the GPU's trace follows the oracle's."""
     x, v, L = ljref.initial_state(864, 0.722, 0.8442, 5489)
@@ -319,7 +319,7 @@ def test_mixed_precision_energy_drift():
 
 
 def test_full_size_properties():
-    """BASELINE config 2 size (N = 1 048 576): size-independent properties."""
+    """At the 1M-atom benchmark size (N = 1 048 576): size-independent properties."""
     from lennardjonesium import initial_condition
     N = 4 * 64 ** 3
     x, v, L = initial_condition(N, 1.0, 0.8442, 5489)
