@@ -422,15 +422,15 @@ build_list_warp_kernel(int N, const double4* __restrict__ pos, const float4* __r
                                         sub = __funnelshift_l(__float_as_uint(sg.y), sub, 1);
                                     }
                                 }
-                                mask |= __brev(sub) >> (24 - t0);
+                                mask |= sub << (24 - t0);  // candidate t at bit 31 - t
                             }
-                            if (cntj < 32) mask &= (1u << cntj) - 1u;  // fillers past the range
+                            if (cntj < 32) mask &= ~(0xffffffffu >> cntj);  // fillers past the range
                             unsigned self = (unsigned)(i - j0);
-                            if (self < 32u) mask &= ~(1u << self);
+                            if (self < 32u) mask &= ~(0x80000000u >> self);
                             if (!own) mask = 0;
-                            while (mask) {
-                                int t = __ffs(mask) - 1;
-                                mask &= mask - 1;
+                            while (mask) {  // hits in ascending slot order
+                                int t = __clz(mask);
+                                mask ^= 0x80000000u >> t;
                                 int j = j0 + t;
                                 // this piece's z offset of slot j: the cell it lies in
                                 int d = pd0[pc];
