@@ -52,6 +52,8 @@ def test_create_rejects_bad_arguments():
     ctx = ctypes.c_void_p()
     p.particle_count = 0
     assert L.lj_gpu_create(ctypes.byref(p), ctypes.byref(ctx)) == _native.LJ_ERR_ARG
+    p.particle_count = 1 << 26  # past the 26-bit slot field of a neighbour entry
+    assert L.lj_gpu_create(ctypes.byref(p), ctypes.byref(ctx)) == _native.LJ_ERR_ARG
     p.particle_count = 10
     for k in range(3):
         p.box[k] = 2.0  # box below the cutoff (particle_pair_filter.cpp:61-64)
