@@ -762,73 +762,84 @@ int lj_batch_create(const lj_batch_system* systems, int nsys, double cutoff, int
     b->nblk = (int)nblk;
     double expect = 4.0 / 3.0 * M_PI * cutmax * cutmax * cutmax * std::max(rho_max, 1.2);
     b->cap = ((int)std::ceil(1.5 * expect + 32) + 3) & ~3;
-    BK(cudaSetDevice(device));
-    BK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-    BK(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking));
-    int N = b->Ntot;
-    std::vector<int> blk_sys((size_t)nblk), blk_first((size_t)nblk), sys_of((size_t)N), cell_sys((size_t)ncell);
-    for (int s = 0; s < nsys; ++s) {
-        const SysDev& S = b->hsys[(size_t)s];
-        for (int j = 0; j < S.nblk; ++j) {
-            blk_sys[(size_t)(S.blk_off + j)] = s;
-            blk_first[(size_t)(S.blk_off + j)] = S.atom_off + j * kThreads;
+    // device set-up; on an error everything allocated so far is released
+    auto init = [&]() -> int {
+        BK(cudaSetDevice(device));
+        BK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+        BK(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking));
+        int N = b->Ntot;
+        std::vector<int> blk_sys((size_t)nblk), blk_first((size_t)nblk), sys_of((size_t)N), cell_sys((size_t)ncell);
+        for (int s = 0; s < nsys; ++s) {
+            const SysDev& S = b->hsys[(size_t)s];
+            for (int j = 0; j < S.nblk; ++j) {
+                blk_sys[(size_t)(S.blk_off + j)] = s;
+                blk_first[(size_t)(S.blk_off + j)] = S.atom_off + j * kThreads;
+            }
+            for (int i = 0; i < S.natoms; ++i) sys_of[(size_t)(S.atom_off + i)] = s;
+            for (int c = 0; c < S.ncell; ++c) cell_sys[(size_t)(S.cell_off + c)] = s;
         }
-        for (int i = 0; i < S.natoms; ++i) sys_of[(size_t)(S.atom_off + i)] = s;
-        for (int c = 0; c < S.ncell; ++c) cell_sys[(size_t)(S.cell_off + c)] = s;
+        BK(cudaMalloc(&b->sys, sizeof(SysDev) * nsys));
+        BK(cudaMalloc(&b->st, sizeof(SysState) * nsys));
+        BK(cudaMalloc(&b->fl, sizeof(BatchFlags)));
+        BK(cudaMalloc(&b->blk_sys, sizeof(int) * nblk));
+        BK(cudaMalloc(&b->blk_first, sizeof(int) * nblk));
+        BK(cudaMalloc(&b->sys_of, sizeof(int) * N));
+        BK(cudaMalloc(&b->cell_sys, sizeof(int) * ncell));
+        BK(cudaMalloc(&b->pos, sizeof(double4) * (N + 1)));
+        BK(cudaMalloc(&b->pos_tmp, sizeof(double4) * N));
+        BK(cudaMalloc(&b->posf, sizeof(float4) * (N + 1)));
+        BK(cudaMalloc(&b->soa, sizeof(double) * SOA_FIELDS * N));
+        BK(cudaMalloc(&b->soa_tmp, sizeof(double) * SOA_FIELDS * N));
+        BK(cudaMalloc(&b->bd, sizeof(double) * 3 * N));
+        BK(cudaMalloc(&b->partials, sizeof(double) * 4 * nblk));
+        BK(cudaMalloc(&b->ring, sizeof(double) * 7 * (size_t)(b->ring_cap + 1) * nsys));
+        BK(cudaMallocHost(&b->host_ring, sizeof(double) * 7 * (size_t)(b->ring_cap + 1) * nsys));
+        BK(cudaMalloc(&b->ids, sizeof(int) * N));
+        BK(cudaMalloc(&b->ids_tmp, sizeof(int) * N));
+        BK(cudaMalloc(&b->cell_of, sizeof(int) * N));
+        BK(cudaMalloc(&b->rank, sizeof(int) * N));
+        BK(cudaMalloc(&b->order, sizeof(int) * N));
+        BK(cudaMalloc(&b->count, sizeof(int) * ncell));
+        BK(cudaMalloc(&b->start, sizeof(int) * (ncell + 1)));
+        BK(cudaMalloc(&b->cnt, sizeof(int) * N));
+        BK(cudaMalloc(&b->nbr, sizeof(uint4) * (size_t)(b->cap / 4) * N));
+        BK(cudaMemcpy(b->sys, b->hsys.data(), sizeof(SysDev) * nsys, cudaMemcpyHostToDevice));
+        std::vector<SysState> st0((size_t)nsys);
+        for (auto& q : st0) {
+            std::memset(&q, 0, sizeof q);
+            q.active = 1;
+            q.need_rebuild = 1;
+        }
+        BK(cudaMemcpy(b->st, st0.data(), sizeof(SysState) * nsys, cudaMemcpyHostToDevice));
+        BK(cudaMemset(b->fl, 0, sizeof(BatchFlags)));
+        BK(cudaMemcpy(b->blk_sys, blk_sys.data(), sizeof(int) * nblk, cudaMemcpyHostToDevice));
+        BK(cudaMemcpy(b->blk_first, blk_first.data(), sizeof(int) * nblk, cudaMemcpyHostToDevice));
+        BK(cudaMemcpy(b->sys_of, sys_of.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+        BK(cudaMemcpy(b->cell_sys, cell_sys.data(), sizeof(int) * ncell, cudaMemcpyHostToDevice));
+        BK(cudaMemset(b->pos, 0, sizeof(double4) * N));
+        BK(cudaMemset(b->soa, 0, sizeof(double) * SOA_FIELDS * N));
+        BK(cudaMemset(b->bd, 0, sizeof(double) * 3 * N));
+        BK(cudaMemset(b->count, 0, sizeof(int) * ncell));
+        BK(cudaMemset(b->cnt, 0, sizeof(int) * N));
+        const double4 ghost = make_double4(1e18, 1e18, 1e18, 0.0);
+        const float4 ghostf = make_float4(1e18f, 1e18f, 1e18f, 0.f);
+        BK(cudaMemcpy(b->pos + N, &ghost, sizeof ghost, cudaMemcpyHostToDevice));
+        BK(cudaMemcpy(b->posf + N, &ghostf, sizeof ghostf, cudaMemcpyHostToDevice));
+        std::vector<int> ident((size_t)N);
+        for (int s = 0; s < nsys; ++s)
+            for (int i = 0; i < b->hsys[(size_t)s].natoms; ++i) ident[(size_t)(b->hsys[(size_t)s].atom_off + i)] = i;
+        BK(cudaMemcpy(b->ids, ident.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+        int sentinel = N;
+        BK(cudaMemcpy(b->start + ncell, &sentinel, sizeof(int), cudaMemcpyHostToDevice));
+        return LJ_OK;
+    };
+    if (int rc = init()) {
+        cudaSetDevice(device);
+        if (b->stream) cudaStreamSynchronize(b->stream);
+        free_b(b);
+        delete b;
+        return rc;
     }
-    BK(cudaMalloc(&b->sys, sizeof(SysDev) * nsys));
-    BK(cudaMalloc(&b->st, sizeof(SysState) * nsys));
-    BK(cudaMalloc(&b->fl, sizeof(BatchFlags)));
-    BK(cudaMalloc(&b->blk_sys, sizeof(int) * nblk));
-    BK(cudaMalloc(&b->blk_first, sizeof(int) * nblk));
-    BK(cudaMalloc(&b->sys_of, sizeof(int) * N));
-    BK(cudaMalloc(&b->cell_sys, sizeof(int) * ncell));
-    BK(cudaMalloc(&b->pos, sizeof(double4) * (N + 1)));
-    BK(cudaMalloc(&b->pos_tmp, sizeof(double4) * N));
-    BK(cudaMalloc(&b->posf, sizeof(float4) * (N + 1)));
-    BK(cudaMalloc(&b->soa, sizeof(double) * SOA_FIELDS * N));
-    BK(cudaMalloc(&b->soa_tmp, sizeof(double) * SOA_FIELDS * N));
-    BK(cudaMalloc(&b->bd, sizeof(double) * 3 * N));
-    BK(cudaMalloc(&b->partials, sizeof(double) * 4 * nblk));
-    BK(cudaMalloc(&b->ring, sizeof(double) * 7 * (size_t)(b->ring_cap + 1) * nsys));
-    BK(cudaMallocHost(&b->host_ring, sizeof(double) * 7 * (size_t)(b->ring_cap + 1) * nsys));
-    BK(cudaMalloc(&b->ids, sizeof(int) * N));
-    BK(cudaMalloc(&b->ids_tmp, sizeof(int) * N));
-    BK(cudaMalloc(&b->cell_of, sizeof(int) * N));
-    BK(cudaMalloc(&b->rank, sizeof(int) * N));
-    BK(cudaMalloc(&b->order, sizeof(int) * N));
-    BK(cudaMalloc(&b->count, sizeof(int) * ncell));
-    BK(cudaMalloc(&b->start, sizeof(int) * (ncell + 1)));
-    BK(cudaMalloc(&b->cnt, sizeof(int) * N));
-    BK(cudaMalloc(&b->nbr, sizeof(uint4) * (size_t)(b->cap / 4) * N));
-    BK(cudaMemcpy(b->sys, b->hsys.data(), sizeof(SysDev) * nsys, cudaMemcpyHostToDevice));
-    std::vector<SysState> st0((size_t)nsys);
-    for (auto& q : st0) {
-        std::memset(&q, 0, sizeof q);
-        q.active = 1;
-        q.need_rebuild = 1;
-    }
-    BK(cudaMemcpy(b->st, st0.data(), sizeof(SysState) * nsys, cudaMemcpyHostToDevice));
-    BK(cudaMemset(b->fl, 0, sizeof(BatchFlags)));
-    BK(cudaMemcpy(b->blk_sys, blk_sys.data(), sizeof(int) * nblk, cudaMemcpyHostToDevice));
-    BK(cudaMemcpy(b->blk_first, blk_first.data(), sizeof(int) * nblk, cudaMemcpyHostToDevice));
-    BK(cudaMemcpy(b->sys_of, sys_of.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
-    BK(cudaMemcpy(b->cell_sys, cell_sys.data(), sizeof(int) * ncell, cudaMemcpyHostToDevice));
-    BK(cudaMemset(b->pos, 0, sizeof(double4) * N));
-    BK(cudaMemset(b->soa, 0, sizeof(double) * SOA_FIELDS * N));
-    BK(cudaMemset(b->bd, 0, sizeof(double) * 3 * N));
-    BK(cudaMemset(b->count, 0, sizeof(int) * ncell));
-    BK(cudaMemset(b->cnt, 0, sizeof(int) * N));
-    const double4 ghost = make_double4(1e18, 1e18, 1e18, 0.0);
-    const float4 ghostf = make_float4(1e18f, 1e18f, 1e18f, 0.f);
-    BK(cudaMemcpy(b->pos + N, &ghost, sizeof ghost, cudaMemcpyHostToDevice));
-    BK(cudaMemcpy(b->posf + N, &ghostf, sizeof ghostf, cudaMemcpyHostToDevice));
-    std::vector<int> ident((size_t)N);
-    for (int s = 0; s < nsys; ++s)
-        for (int i = 0; i < b->hsys[(size_t)s].natoms; ++i) ident[(size_t)(b->hsys[(size_t)s].atom_off + i)] = i;
-    BK(cudaMemcpy(b->ids, ident.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
-    int sentinel = N;
-    BK(cudaMemcpy(b->start + ncell, &sentinel, sizeof(int), cudaMemcpyHostToDevice));
     *out = b;
     return LJ_OK;
 }

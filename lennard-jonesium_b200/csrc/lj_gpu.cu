@@ -526,53 +526,9 @@ void free_all(lj_ctx* c) {
     if (c->stream) cudaStreamDestroy(c->stream);
 }
 
-}  // namespace
-
-extern "C" {
-
-void lj_gpu_default_params(lj_params* p) {
-    if (!p) return;
-    std::memset(p, 0, sizeof *p);
-    p->particle_count = 0;
-    p->box[0] = p->box[1] = p->box[2] = 1.0;
-    p->cutoff_distance = 2.5;
-    p->time_delta = 0.005;
-    p->precision = LJ_PRECISION_FP64;
-    p->force_kind = LJ_FORCE_LJ;
-    p->force_strength = 0.0;
-    p->periodic = 1;
-    p->device = 0;
-    p->skin = -1.0;
-    p->neighbor_capacity = 0;
-}
-
-const char* lj_gpu_status_string(int s) {
-    return (s >= 0 && s <= 5) ? kStatus[s] : "unknown status";
-}
-
-const char* lj_gpu_last_error(const lj_ctx* ctx) { return ctx ? ctx->err : "null context"; }
-
-int lj_gpu_create(const lj_params* params, lj_ctx** out) {
-    lj_ctx* ctx = nullptr;
-    if (!params || !out) return LJ_ERR_ARG;
-    *out = nullptr;
-    const lj_params& p = *params;
-    if (p.particle_count < 1 || p.particle_count >= kMaxAtoms) return LJ_ERR_ARG;
-    if (!(p.cutoff_distance > 0) || !(p.time_delta >= 0)) return LJ_ERR_ARG;
-    for (int k = 0; k < 3; ++k) {
-        if (!(p.box[k] > 0) || !std::isfinite(p.box[k])) return LJ_ERR_ARG;
-        // particle_pair_filter.cpp:61-64 -- only a pair filter needs box >= rc
-        if (p.force_kind != LJ_FORCE_NONE && !(p.box[k] >= p.cutoff_distance)) return LJ_ERR_ARG;
-    }
-    if (p.force_kind < LJ_FORCE_NONE || p.force_kind > LJ_FORCE_CONSTANT) return LJ_ERR_ARG;
-    if (p.precision != LJ_PRECISION_FP64 && p.precision != LJ_PRECISION_MIXED) return LJ_ERR_ARG;
-    if (!p.periodic && p.force_kind != LJ_FORCE_NONE) return LJ_ERR_ARG;
-    // lennard_jones_force.cpp:45 -- the cutoff must lie beyond the potential minimum
-    if (p.force_kind == LJ_FORCE_LJ && !(p.cutoff_distance * p.cutoff_distance > std::cbrt(2.0)))
-        return LJ_ERR_ARG;
-
-    ctx = new (std::nothrow) lj_ctx();
-    if (!ctx) return LJ_ERR_ARG;
+// Everything of lj_gpu_create past the host-side argument checks; on an error
+// the caller releases what was allocated.
+int init_ctx(lj_ctx* ctx, const lj_params& p) {
     ctx->p = p;
     int N = ctx->N = p.particle_count;
     CK(cudaSetDevice(p.device));
@@ -609,7 +565,6 @@ int lj_gpu_create(const lj_params* params, lj_ctx** out) {
     ctx->small_box = std::min(ctx->list_grid.n[0], std::min(ctx->list_grid.n[1], ctx->list_grid.n[2])) < 3;
     ctx->rebuild_always = skin == 0.0;
     if (ctx->list_grid.ncell() > kScanTile * kMaxScanTiles || ctx->ref_grid.ncell() > kScanTile * kMaxScanTiles) {
-        delete ctx;
         return LJ_ERR_ARG;
     }
 
@@ -623,13 +578,11 @@ int lj_gpu_create(const lj_params* params, lj_ctx** out) {
     ctx->cap = cap;
     ctx->nblocks = blocks_for(N);
     if (p.force_block != 0 && p.force_block != 64 && p.force_block != 128 && p.force_block != 256) {
-        delete ctx;
         return LJ_ERR_ARG;
     }
     ctx->force_block = p.force_block ? p.force_block : 128;
     ctx->fblocks = blocks_for(N, ctx->force_block);
     if (p.tile_cells < 0 || p.tile_cells > kTileMaxRun || p.tile_capacity < 0 || p.tile_capacity > kTileMaxSmemAtoms) {
-        delete ctx;
         return LJ_ERR_ARG;
     }
     // mixed path over shared-memory tiles: runs of tile_cells list cells per
@@ -716,6 +669,64 @@ int lj_gpu_create(const lj_params* params, lj_ctx** out) {
     int one = 1;
     CK(cudaMemcpyAsync(&ctx->sc->need_rebuild, &one, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    return LJ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void lj_gpu_default_params(lj_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof *p);
+    p->particle_count = 0;
+    p->box[0] = p->box[1] = p->box[2] = 1.0;
+    p->cutoff_distance = 2.5;
+    p->time_delta = 0.005;
+    p->precision = LJ_PRECISION_FP64;
+    p->force_kind = LJ_FORCE_LJ;
+    p->force_strength = 0.0;
+    p->periodic = 1;
+    p->device = 0;
+    p->skin = -1.0;
+    p->neighbor_capacity = 0;
+}
+
+const char* lj_gpu_status_string(int s) {
+    return (s >= 0 && s <= 5) ? kStatus[s] : "unknown status";
+}
+
+const char* lj_gpu_last_error(const lj_ctx* ctx) { return ctx ? ctx->err : "null context"; }
+
+int lj_gpu_create(const lj_params* params, lj_ctx** out) {
+    lj_ctx* ctx = nullptr;
+    if (!params || !out) return LJ_ERR_ARG;
+    *out = nullptr;
+    const lj_params& p = *params;
+    if (p.particle_count < 1 || p.particle_count >= kMaxAtoms) return LJ_ERR_ARG;
+    if (!(p.cutoff_distance > 0) || !(p.time_delta >= 0)) return LJ_ERR_ARG;
+    for (int k = 0; k < 3; ++k) {
+        if (!(p.box[k] > 0) || !std::isfinite(p.box[k])) return LJ_ERR_ARG;
+        // particle_pair_filter.cpp:61-64 -- only a pair filter needs box >= rc
+        if (p.force_kind != LJ_FORCE_NONE && !(p.box[k] >= p.cutoff_distance)) return LJ_ERR_ARG;
+    }
+    if (p.force_kind < LJ_FORCE_NONE || p.force_kind > LJ_FORCE_CONSTANT) return LJ_ERR_ARG;
+    if (p.precision != LJ_PRECISION_FP64 && p.precision != LJ_PRECISION_MIXED) return LJ_ERR_ARG;
+    if (!p.periodic && p.force_kind != LJ_FORCE_NONE) return LJ_ERR_ARG;
+    // lennard_jones_force.cpp:45 -- the cutoff must lie beyond the potential minimum
+    if (p.force_kind == LJ_FORCE_LJ && !(p.cutoff_distance * p.cutoff_distance > std::cbrt(2.0)))
+        return LJ_ERR_ARG;
+
+    ctx = new (std::nothrow) lj_ctx();
+    if (!ctx) return LJ_ERR_ARG;
+    int rc = init_ctx(ctx, p);
+    if (rc) {
+        cudaSetDevice(p.device);
+        if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+        free_all(ctx);
+        delete ctx;
+        return rc;
+    }
     *out = ctx;
     return LJ_OK;
 }
