@@ -26,6 +26,14 @@
 
 using namespace ljb;
 
+// One instantiated step graph.
+struct StepGraph {
+    cudaGraphExec_t exec = nullptr;
+    int steps = 0;          // steps per launch
+    int kernels = 0;        // kernel nodes outside the rebuild bodies
+    long long launches = 0;
+};
+
 struct lj_ctx {
     lj_params p{};
     int N = 0;
@@ -90,12 +98,11 @@ struct lj_ctx {
 
     long long launches = 0;       // kernels launched directly (gated-off ones included)
     long long host_steps = 0;     // mirror of the device step counter
-    // step graphs: kick_drift -> decide -> IF(rebuild chain) -> force -> finalize, unrolled
+    // step graphs: kick_drift -> decide -> IF(rebuild chain) -> force -> finalize, unrolled;
+    // a long one for runs of steps and a short one for the remainder
     cudaStream_t side = nullptr;  // captures the conditional body
-    cudaGraphExec_t graph_k = nullptr;
-    int graph_steps = 0;          // steps per graph launch (0: graphs unavailable)
+    StepGraph graphs[2];
     bool graph_tried = false;
-    long long graph_launched_steps = 0;
     int rebuild_kernels = 0;      // kernels in one rebuild chain
     char err[512] = {0};
 };
@@ -345,28 +352,33 @@ int launch_step(lj_ctx* ctx) {
         CKL();
     }
     finalize_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->partials, partial_blocks(ctx, forces), ctx->N, ctx->pp.dt, 0,
-                                                 forces ? 1 : 0, ctx->sc, ctx->ring, ctx->ring_cap);
+                                                 forces ? 1 : 0, ctx->sc, ctx->ring, ctx->ring_cap, NextStep{});
     CKL();
     return LJ_OK;
 }
 
 // Capture `nsteps` steps into one executable graph.  Each step is
-//   kick_drift -> decide -> IF(rebuild chain) -> force(+kick) -> finalize
-// where `decide` sets the conditional from the device-side gate, so the
+//   kick_drift -> [decide] -> IF(rebuild chain) -> force(+kick) -> finalize
+// where the conditional is set on the device from the rebuild gate, so the
 // rebuild kernels are not even launched on the steps that do not need them.
+// The gate reads the displacement of the step's own positions: with fused
+// steps the previous step's pair kernel computed it and that step's finalize
+// sets the conditional; otherwise (and on the first step) a one-thread
+// `decide` kernel after kick_drift does.
 // With an even step count the pair kernels of all but the last step also run
 // the next step's kick and drift (Fuse), alternating between the two position
 // buffers: kick_drift only opens the graph (writing the second buffer) and the
 // last, unfused step leaves the state in the first buffer again.
-// Returns LJ_OK with ctx->graph_k set, or an error (the caller then keeps
+// Returns LJ_OK with `out` filled, or an error (the caller then keeps
 // launching the steps one kernel at a time).
-int build_step_graph(lj_ctx* ctx, int nsteps) {
+int build_step_graph(lj_ctx* ctx, int nsteps, StepGraph& out) {
     cudaStream_t main = ctx->stream;
     long long launches0 = ctx->launches;
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamBeginCapture(main, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return set_err(ctx, LJ_ERR_CUDA, cudaGetErrorString(e));
     int rc = LJ_OK;
+    int kernels = 0;
     bool forces = ctx->p.force_kind != LJ_FORCE_NONE;
     bool fuse = forces && can_fuse(ctx) && nsteps % 2 == 0;
     double4* const posA = ctx->pos;
@@ -375,39 +387,49 @@ int build_step_graph(lj_ctx* ctx, int nsteps) {
         x = ctx->pos == posA ? ctx->pos_b : posA;
         xl = ctx->posl == poslA ? ctx->posl_b : poslA;
     };
+    auto new_handle = [&](cudaGraphConditionalHandle& h) -> bool {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t g = nullptr;
+        return (e = cudaStreamGetCaptureInfo(main, &cs, nullptr, &g, nullptr, nullptr)) == cudaSuccess &&
+               (e = cudaGraphConditionalHandleCreate(&h, g, 0, 0)) == cudaSuccess;
+    };
+    cudaGraphConditionalHandle h = 0;  // this step's rebuild conditional
     for (int st = 0; st < nsteps && rc == LJ_OK; ++st) {
         if (!fuse) {
             rc = launch_kick_drift(ctx);
+            ++kernels;
         } else if (st == 0) {
             rc = launch_kick_drift(ctx, ctx->pos_b, ctx->posl_b);
+            ++kernels;
             ctx->pos = ctx->pos_b;
             ctx->posl = ctx->posl_b;
         }
         if (rc) break;
         if (forces) {
+            if (st == 0 || !fuse) {
+                if (!new_handle(h)) {
+                    rc = LJ_ERR_CUDA;
+                    break;
+                }
+                decide_rebuild_kernel<<<1, 1, 0, main>>>(gate_of(ctx), h, ctx->sc);
+                ++kernels;
+                if ((e = cudaGetLastError()) != cudaSuccess) {
+                    rc = LJ_ERR_CUDA;
+                    break;
+                }
+            }
             cudaStreamCaptureStatus cs;
             cudaGraph_t g = nullptr;
             const cudaGraphNode_t* deps = nullptr;
             size_t ndeps = 0;
-            cudaGraphConditionalHandle h;
-            if ((e = cudaStreamGetCaptureInfo(main, &cs, nullptr, &g, &deps, &ndeps)) != cudaSuccess ||
-                (e = cudaGraphConditionalHandleCreate(&h, g, 0, 0)) != cudaSuccess) {
-                rc = LJ_ERR_CUDA;
-                break;
-            }
-            decide_rebuild_kernel<<<1, 1, 0, main>>>(gate_of(ctx), h, ctx->sc);
-            if ((e = cudaGetLastError()) != cudaSuccess ||
-                (e = cudaStreamGetCaptureInfo(main, &cs, nullptr, &g, &deps, &ndeps)) != cudaSuccess) {
-                rc = LJ_ERR_CUDA;
-                break;
-            }
             cudaGraphNodeParams cp = {};
             cp.type = cudaGraphNodeTypeConditional;
             cp.conditional.handle = h;
             cp.conditional.type = cudaGraphCondTypeIf;
             cp.conditional.size = 1;
             cudaGraphNode_t cnode;
-            if ((e = cudaGraphAddNode(&cnode, g, deps, ndeps, &cp)) != cudaSuccess ||
+            if ((e = cudaStreamGetCaptureInfo(main, &cs, nullptr, &g, &deps, &ndeps)) != cudaSuccess ||
+                (e = cudaGraphAddNode(&cnode, g, deps, ndeps, &cp)) != cudaSuccess ||
                 (e = cudaStreamUpdateCaptureDependencies(main, &cnode, 1, cudaStreamSetCaptureDependencies)) !=
                     cudaSuccess) {
                 rc = LJ_ERR_CUDA;
@@ -439,15 +461,25 @@ int build_step_graph(lj_ctx* ctx, int nsteps) {
             } else {
                 rc = launch_force(ctx, true);
             }
+            ++kernels;
         } else {
             kick_measure_kernel<<<ctx->nblocks, kThreads, 0, main>>>(ctx->N, soa_of(ctx->soa, ctx->N), ctx->pp.dt, 1,
                                                                      ctx->partials);
+            ++kernels;
             if (cudaGetLastError() != cudaSuccess) rc = LJ_ERR_CUDA;
         }
         if (rc) break;
+        NextStep next{};
+        if (forces && fuse && st + 1 < nsteps) {
+            if (!new_handle(h)) {  // the next step's conditional, set by this finalize
+                rc = LJ_ERR_CUDA;
+                break;
+            }
+            next = NextStep{gate_of(ctx), h, 1};
+        }
         finalize_kernel<<<1, 1024, 0, main>>>(ctx->partials, partial_blocks(ctx, forces), ctx->N, ctx->pp.dt, 0,
-                                              forces ? 1 : 0,
-                                              ctx->sc, ctx->ring, ctx->ring_cap);
+                                              forces ? 1 : 0, ctx->sc, ctx->ring, ctx->ring_cap, next);
+        ++kernels;
         if (cudaGetLastError() != cudaSuccess) rc = LJ_ERR_CUDA;
         if (fuse && st + 1 < nsteps) {
             double4* nx = nullptr;
@@ -468,31 +500,38 @@ int build_step_graph(lj_ctx* ctx, int nsteps) {
         rc = LJ_ERR_CUDA;
     }
     if (rc == LJ_OK) {
-        e = cudaGraphInstantiate(&ctx->graph_k, graph, 0);
+        e = cudaGraphInstantiate(&out.exec, graph, 0);
         if (e != cudaSuccess) rc = LJ_ERR_CUDA;
     }
     if (graph) cudaGraphDestroy(graph);
     if (rc) {
-        ctx->graph_k = nullptr;
+        out.exec = nullptr;
         std::snprintf(ctx->err, sizeof ctx->err, "step graph unavailable: %s", cudaGetErrorString(e));
         cudaGetLastError();  // clear the sticky-free error state of the failed capture
+    } else {
+        out.steps = nsteps;
+        out.kernels = kernels;
     }
     return rc;
 }
 
-constexpr int kGraphSteps = 8;
+// Steps per launch of the two step graphs: the long one amortises the
+// graph-opening kick_drift over more steps.
+constexpr int kGraphSteps[2] = {32, 8};
 
 // Enqueue nsteps steps: whole step graphs where available, single launches for the rest.
 int enqueue_steps(lj_ctx* ctx, int nsteps) {
     if (!ctx->graph_tried) {
         ctx->graph_tried = true;
-        if (build_step_graph(ctx, kGraphSteps) == LJ_OK) ctx->graph_steps = kGraphSteps;
+        for (int q = 0; q < 2; ++q)
+            if (build_step_graph(ctx, kGraphSteps[q], ctx->graphs[q]) != LJ_OK) break;
     }
     int s = 0;
-    if (ctx->graph_steps > 0) {
-        for (; s + ctx->graph_steps <= nsteps; s += ctx->graph_steps) {
-            CK(cudaGraphLaunch(ctx->graph_k, ctx->stream));
-            ctx->graph_launched_steps += ctx->graph_steps;
+    for (StepGraph& g : ctx->graphs) {
+        if (!g.exec) break;
+        for (; s + g.steps <= nsteps; s += g.steps) {
+            CK(cudaGraphLaunch(g.exec, ctx->stream));
+            ++g.launches;
         }
     }
     for (; s < nsteps; ++s) {
@@ -521,7 +560,8 @@ void free_all(lj_ctx* c) {
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (c->host_ring) cudaFreeHost(c->host_ring);
-    if (c->graph_k) cudaGraphExecDestroy(c->graph_k);
+    for (StepGraph& g : c->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
     if (c->side) cudaStreamDestroy(c->side);
     if (c->stream) cudaStreamDestroy(c->stream);
 }
@@ -817,7 +857,7 @@ int lj_gpu_compute_forces(lj_ctx* ctx, double* pe, double* virial) {
         rc = launch_force(ctx, false);
         if (rc) return rc;
         finalize_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->partials, partial_blocks(ctx, true), ctx->N, ctx->pp.dt, 1, 1,
-                                                     ctx->sc, ctx->ring, ctx->ring_cap);
+                                                     ctx->sc, ctx->ring, ctx->ring_cap, NextStep{});
         CKL();
     }
     int rc = read_flags(ctx);
@@ -864,7 +904,7 @@ int lj_gpu_measure(lj_ctx* ctx, lj_thermo* out) {
                                                                      ctx->partials);
     CKL();
     finalize_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->partials, ctx->nblocks, ctx->N, ctx->pp.dt, 2, 0,
-                                                 ctx->sc, ctx->ring, ctx->ring_cap);
+                                                 ctx->sc, ctx->ring, ctx->ring_cap, NextStep{});
     CKL();
     CK(cudaMemcpyAsync(ctx->host_ring, ctx->ring + 7 * (size_t)ctx->ring_cap, sizeof(double) * 7,
                        cudaMemcpyDeviceToHost, ctx->stream));
@@ -994,9 +1034,10 @@ int lj_gpu_get_stats(const lj_ctx* ctx_c, lj_stats* out) {
     out->max_neighbors = h.max_count;
     out->small_box = ctx->small_box ? 1 : 0;
     out->skin = ctx->skin;
-    // direct launches + kernel nodes executed by step graphs (kick, decide, force,
-    // finalize per step, and the rebuild chain each time the conditional opened)
-    out->kernel_launches = ctx->launches + 4 * ctx->graph_launched_steps + (long long)ctx->rebuild_kernels * h.graph_rebuilds;
+    // direct launches + kernel nodes executed by step graphs (each launch's
+    // kernels, and the rebuild chain each time a conditional opened)
+    out->kernel_launches = ctx->launches + (long long)ctx->rebuild_kernels * h.graph_rebuilds;
+    for (const StepGraph& g : ctx->graphs) out->kernel_launches += g.launches * g.kernels;
     out->tile_cells = ctx->tiles ? ctx->tile_cells : 0;
     out->tile_capacity = ctx->tiles ? ctx->tg.cap : 0;
     out->max_staged = h.max_staged;
@@ -1054,7 +1095,7 @@ int lj_gpu_step_timed(lj_ctx* ctx, int nsteps, lj_phase_times* out) {
         }
         CK(cudaEventRecord(ev[3], ctx->stream));
         finalize_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->partials, partial_blocks(ctx, forces), ctx->N, ctx->pp.dt,
-                                                     0, forces ? 1 : 0, ctx->sc, ctx->ring, ctx->ring_cap);
+                                                     0, forces ? 1 : 0, ctx->sc, ctx->ring, ctx->ring_cap, NextStep{});
         CKL();
         CK(cudaEventRecord(ev[4], ctx->stream));
         CK(cudaEventSynchronize(ev[4]));

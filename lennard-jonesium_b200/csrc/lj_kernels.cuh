@@ -666,9 +666,18 @@ force_fp64_kernel(int N, const double4* __restrict__ pos, Soa s, const uint4* __
 // mode 0: after a step (t += dt); 1: after a force evaluation (PE, W only);
 // 2: measurement of the current state.
 // ---------------------------------------------------------------------------
+// Step graphs: the finalize of a step also takes the next step's rebuild
+// decision (the conditional handle of the next step's rebuild node), saving
+// that step a one-thread launch.
+struct NextStep {
+    Gate gate;
+    cudaGraphConditionalHandle h;
+    int set;  // 0: no next step in this graph
+};
+
 static __global__ void __launch_bounds__(1024)
 finalize_kernel(const double* __restrict__ partials, int nblocks, int N, double dt, int mode,
-                int forces_valid, Scalars* sc, double* __restrict__ ring, int ring_cap) {
+                int forces_valid, Scalars* sc, double* __restrict__ ring, int ring_cap, NextStep next) {
     // each thread sums blocks tid, tid + 1024, ... in that order; eight blocks'
     // partials (32-byte loads) are in flight at a time
     double acc[4] = {0, 0, 0, 0};
@@ -723,6 +732,11 @@ finalize_kernel(const double* __restrict__ partials, int nblocks, int N, double 
             sc->max_disp2 = sc->max_disp2_next;
             sc->max_disp2_next = 0ull;
             sc->need_rebuild = 0;
+        }
+        if (next.set) {
+            bool open = next.gate.open();
+            if (open) sc->graph_rebuilds += 1;
+            cudaGraphSetConditional(next.h, open ? 1u : 0u);
         }
     }
 }

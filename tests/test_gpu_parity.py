@@ -378,8 +378,8 @@ def test_graph_steps_equal_direct_launches(precision):
     with gpu_system(4000, L, precision=precision) as a, gpu_system(4000, L, precision=precision) as b:
         a.upload(x, v=v)
         b.upload(x, v=v)
-        ra = a.step(64)           # 8 graph launches of 8 steps
-        b.step_timed(64)          # direct launches with per-phase events
+        ra = a.step(72)           # two launches of the 32-step graph, one of the 8-step graph
+        b.step_timed(72)          # direct launches with per-phase events
         rb = b.step(1)            # one more step on both to compare a record
         ra1 = a.step(1)
         sa, sb = a.download(), b.download()
