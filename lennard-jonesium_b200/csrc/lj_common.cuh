@@ -6,6 +6,7 @@
 // into FMAs; the CPU oracle (oracle/ljref.cpp) uses the same fixed order.
 #pragma once
 
+#include <climits>
 #include <cstdint>
 #include <cuda_runtime.h>
 

@@ -329,12 +329,16 @@ build_list_kernel(int N, const double4* __restrict__ pos, const float4* __restri
 // negated as separate x / y / z rows); every lane tests the staged candidates
 // through broadcast reads, two per instruction with Blackwell's packed FP32x2
 // add / multiply / fma, in unrolled blocks of 8 that only set bits of a hit
-// mask.  A short per-lane loop over the set bits then appends the entries, so
-// the append code is not issued once per candidate.  Each lane collects entries
-// in a 4-entry shared buffer and writes whole groups (one 16-byte store).
-// Entries, their order (stencil cell, then slot) and the candidate radius are
-// those of build_list_kernel<false>.
+// mask.  The masks of up to kBuildRecords chunks are kept in shared memory
+// (with each chunk's first slot, entry code and the slots where the code's z
+// offset steps up) and then appended in one per-lane loop over all their set
+// bits: the warp runs as many append rounds as its busiest lane has hits,
+// instead of the busiest lane's hits in every chunk added up.  Each lane
+// collects entries in a 4-entry shared buffer and writes whole groups (one
+// 16-byte store).  Entries, their order (stencil cell, then slot) and the
+// candidate radius are those of build_list_kernel<false>.
 constexpr int kBuildWarps = 4;
+constexpr int kBuildRecords = 24;
 
 __device__ __forceinline__ void append_entry(unsigned (&grp)[4], int& n, int cap, unsigned entry,
                                              uint4* __restrict__ nbr4, size_t N, int i) {
@@ -352,6 +356,10 @@ build_list_warp_kernel(int N, const double4* __restrict__ pos, const float4* __r
     if (!gate.open()) return;
     __shared__ __align__(16) float cxs[kBuildWarps][3][32];
     __shared__ unsigned grp_s[kBuildWarps][32][4];
+    __shared__ unsigned rec_mask[kBuildWarps][kBuildRecords][32];
+    // per chunk: first slot, entry code of its first cell, slots where the z
+    // offset of the code steps up by one (INT_MAX: none)
+    __shared__ int4 rec_meta[kBuildWarps][kBuildRecords];
     int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int c = blockIdx.x * kBuildWarps + warp;
     int ncell = g.ncell();
@@ -375,6 +383,30 @@ build_list_warp_kernel(int N, const double4* __restrict__ pos, const float4* __r
             bool own = i < he;
             float4 xi = own ? posf[i] : make_float4(0.f, 0.f, 0.f, 0.f);
             int n = 0;
+            int nrec = 0;  // chunk records waiting to be appended (warp-uniform)
+            // append the hits of the recorded chunks in order: one round per hit
+            // of this lane, a round that finds the current mask empty first moves
+            // on to the next record
+            auto flush = [&]() {
+                __syncwarp();
+                int k = 0;
+                unsigned m = rec_mask[warp][0][lane];
+                int4 meta = rec_meta[warp][0];
+                for (;;) {
+                    while (m == 0 && ++k < nrec) {
+                        m = rec_mask[warp][k][lane];
+                        meta = rec_meta[warp][k];
+                    }
+                    if (m == 0) break;
+                    int t = __clz(m);
+                    m ^= 0x80000000u >> t;
+                    int j = meta.x + t;
+                    unsigned code = (unsigned)meta.y + (j >= meta.z ? 16u : 0u) + (j >= meta.w ? 16u : 0u);
+                    append_entry(grp, n, cap, make_entry((unsigned)j, code), nbr4, N, i);
+                }
+                __syncwarp();
+                nrec = 0;
+            };
             for (int a = -1; a <= 1; ++a) {
                 int na = ca + a, ia = na < 0 ? -1 : (na >= g.n[0] ? 1 : 0);
                 na -= ia * g.n[0];
@@ -428,20 +460,23 @@ build_list_warp_kernel(int N, const double4* __restrict__ pos, const float4* __r
                             unsigned self = (unsigned)(i - j0);
                             if (self < 32u) mask &= ~(0x80000000u >> self);
                             if (!own) mask = 0;
-                            while (mask) {  // hits in ascending slot order
-                                int t = __clz(mask);
-                                mask ^= 0x80000000u >> t;
-                                int j = j0 + t;
-                                // this piece's z offset of slot j: the cell it lies in
-                                int d = pd0[pc];
-                                if (d < 0 && pd1[pc] >= 0 && j >= s0) d = 0;
-                                if (d < 1 && pd1[pc] >= 1 && j >= s1) d = 1;
-                                append_entry(grp, n, cap, make_entry((unsigned)j, offset_code(a, b, d)), nbr4, N, i);
+                            if (__any_sync(0xffffffffu, mask != 0u)) {
+                                rec_mask[warp][nrec][lane] = mask;
+                                if (lane == 0) {
+                                    // the piece's z offsets: slot j lies in the cell
+                                    // d = pd0 + (j >= s0 if the piece holds d = 0) + ...
+                                    int dl = pd0[pc], dh = pd1[pc];
+                                    rec_meta[warp][nrec] =
+                                        make_int4(j0, (int)offset_code(a, b, dl), dl < 0 && dh >= 0 ? s0 : INT_MAX,
+                                                  dl < 1 && dh >= 1 ? s1 : INT_MAX);
+                                }
+                                if (++nrec == kBuildRecords) flush();
                             }
                         }
                     }
                 }
             }
+            if (nrec) flush();
             if (own) {
                 int m = n < cap ? n : cap;
                 cnt[i] = m;
