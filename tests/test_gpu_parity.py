@@ -22,6 +22,7 @@ FCC_CASES = [  # N, T, rho, seed, rc
     (500, 0.5, 0.8, 117208264, 2.5),
     (100, 0.6, 1.0, 17, 2.0),       # 2 cells per axis (the reference's Python test config)
     (4000, 1.2, 0.8, 7, 2.5),
+    (4000, 1.2, 0.8, 7, 4.5),       # 3 list cells of ~5.7 sigma per axis: the largest cell edges
 ]
 
 
