@@ -237,13 +237,14 @@ b_copy_back_kernel(const int* __restrict__ sys_of, const SysState* st, int Ntot,
     ids[k] = ids_in[k];
 }
 
-// Warp-per-cell list build (the algorithm of build_list_warp_kernel, per system).
-static __global__ void __launch_bounds__(32 * kBuildWarps)
+// Warp-per-cell list build: the per-cell body of build_list_warp_kernel, on
+// the grid and slot ranges of the cell's own system (entries identical to a
+// single-system build of that system).
+static __global__ void __launch_bounds__(32 * kBuildWarps, 6)
 b_build_list_kernel(const int* __restrict__ cell_sys, const SysDev* __restrict__ sys, SysState* st, int ncell_tot,
                     int Ntot, const float4* __restrict__ posf, const int* __restrict__ start, int cap,
                     uint4* __restrict__ nbr4, int* __restrict__ cnt, BatchFlags* fl) {
-    __shared__ __align__(16) float cxs[kBuildWarps][3][32];
-    __shared__ unsigned grp_s[kBuildWarps][32][4];
+    __shared__ BuildSmem bs[kBuildWarps];
     int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int c = blockIdx.x * kBuildWarps + warp;
     if (c >= ncell_tot) return;
@@ -252,71 +253,8 @@ b_build_list_kernel(const int* __restrict__ cell_sys, const SysDev* __restrict__
     const SysDev& S = sys[sidx];
     const Grid& g = S.grid;
     int lc = c - S.cell_off;
-    int ca = lc / (g.n[1] * g.n[2]), cb = (lc / g.n[2]) % g.n[1], cc = lc % g.n[2];
-    int hs = start[c], he = start[c + 1];
-    unsigned (&grp)[4] = grp_s[warp][lane];
-    int wmax = 0;
-    for (int h0 = hs; h0 < he; h0 += 32) {
-        int i = h0 + lane;
-        bool own = i < he;
-        float4 xi = own ? posf[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-        int n = 0;
-        for (int a = -1; a <= 1; ++a) {
-            int na = ca + a, ia = na < 0 ? -1 : (na >= g.n[0] ? 1 : 0);
-            na -= ia * g.n[0];
-            for (int b = -1; b <= 1; ++b) {
-                int nb = cb + b, ib = nb < 0 ? -1 : (nb >= g.n[1] ? 1 : 0);
-                nb -= ib * g.n[1];
-                for (int d = -1; d <= 1; ++d) {
-                    int nc = cc + d, ic = nc < 0 ? -1 : (nc >= g.n[2] ? 1 : 0);
-                    nc -= ic * g.n[2];
-                    int cell = S.cell_off + g.flat(na, nb, nc);
-                    float2 sx = make_float2(xi.x - ia * S.Lf.x, xi.x - ia * S.Lf.x);
-                    float2 sy = make_float2(xi.y - ib * S.Lf.y, xi.y - ib * S.Lf.y);
-                    float2 sz = make_float2(xi.z - ic * S.Lf.z, xi.z - ic * S.Lf.z);
-                    unsigned code = offset_code(a, b, d);
-                    int js = start[cell], je = start[cell + 1];
-                    for (int j0 = js; j0 < je; j0 += 32) {
-                        int cntj = min(32, je - j0);
-                        __syncwarp();
-                        float4 q = lane < cntj ? posf[j0 + lane] : make_float4(1e18f, 1e18f, 1e18f, 0.f);
-                        cxs[warp][0][lane] = -q.x;
-                        cxs[warp][1][lane] = -q.y;
-                        cxs[warp][2][lane] = -q.z;
-                        __syncwarp();
-                        unsigned mask = 0;
-                        for (int t = 0; t < cntj; t += 2) {
-                            float2 qx = *reinterpret_cast<const float2*>(&cxs[warp][0][t]);
-                            float2 qy = *reinterpret_cast<const float2*>(&cxs[warp][1][t]);
-                            float2 qz = *reinterpret_cast<const float2*>(&cxs[warp][2][t]);
-                            float2 dx = __fadd2_rn(sx, qx), dy = __fadd2_rn(sy, qy), dz = __fadd2_rn(sz, qz);
-                            float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-                            mask |= (r2.x < S.cut2 ? 1u : 0u) << t;
-                            mask |= (r2.y < S.cut2 ? 2u : 0u) << t;
-                        }
-                        if (cntj < 32) mask &= (1u << cntj) - 1u;
-                        unsigned self = (unsigned)(i - j0);
-                        if (self < 32u) mask &= ~(1u << self);
-                        if (!own) mask = 0;
-                        while (mask) {
-                            int t = __ffs(mask) - 1;
-                            mask &= mask - 1;
-                            append_entry(grp, n, cap, make_entry((unsigned)(j0 + t), code), nbr4, Ntot, i);
-                        }
-                    }
-                }
-            }
-        }
-        if (own) {
-            int m = n < cap ? n : cap;
-            cnt[i] = m;
-            if (m & 3) {
-                for (int k = m & 3; k < 4; ++k) grp[k] = make_entry((unsigned)Ntot, kGhostCode);
-                nbr4[(size_t)(m >> 2) * Ntot + i] = make_uint4(grp[0], grp[1], grp[2], grp[3]);
-            }
-            wmax = max(wmax, n);
-        }
-    }
+    int wmax = build_cell_lists(lc / (g.n[1] * g.n[2]), (lc / g.n[2]) % g.n[1], lc % g.n[2], g, start + S.cell_off,
+                                posf, S.Lf, S.cut2, cap, nbr4, cnt, Ntot, bs[warp], lane);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) wmax = max(wmax, __shfl_down_sync(0xffffffffu, wmax, off));
     if (lane == 0 && wmax > cap) atomicExch(&fl->overflow, 1);

@@ -349,145 +349,164 @@ __device__ __forceinline__ void append_entry(unsigned (&grp)[4], int& n, int cap
     ++n;
 }
 
+// Shared memory of one list-building warp: the staged candidates, each lane's
+// 4-entry group buffer and the chunk records waiting to be appended (per
+// chunk: first slot, entry code of its first cell, slots where the z offset
+// of the code steps up by one -- INT_MAX: none).
+struct __align__(16) BuildSmem {
+    float cxs[3][32];
+    unsigned grp[32][4];
+    unsigned rec_mask[kBuildRecords][32];
+    int4 rec_meta[kBuildRecords];
+};
+
+// One warp builds the lists of the atoms of list cell (ca, cb, cc) of grid g
+// (>= 3 cells per axis).  `start` holds the slot ranges of the grid's cells
+// (slots are global: N is the list stride and the ghost slot).  Returns the
+// largest list length of the warp's lanes (before the capacity cut).
+__device__ __forceinline__ int build_cell_lists(int ca, int cb, int cc, const Grid& g, const int* __restrict__ start,
+                                                const float4* __restrict__ posf, float3 Lf, float cut2, int cap,
+                                                uint4* __restrict__ nbr4, int* __restrict__ cnt, int N,
+                                                BuildSmem& sm, int lane) {
+    int wmax = 0;
+    unsigned(&grp)[4] = sm.grp[lane];
+    int nz = g.n[2];
+    // the column's z cells d = -1, 0, 1 as at most two contiguous pieces,
+    // split where the column wraps (each piece has one z image)
+    int npc = 1, pd0[2] = {-1, 0}, pd1[2] = {1, 1}, pic[2] = {0, 0};
+    if (cc == 0) {
+        npc = 2; pd0[0] = -1; pd1[0] = -1; pic[0] = -1; pd0[1] = 0; pd1[1] = 1; pic[1] = 0;
+    } else if (cc == nz - 1) {
+        npc = 2; pd0[0] = -1; pd1[0] = 0; pic[0] = 0; pd0[1] = 1; pd1[1] = 1; pic[1] = 1;
+    }
+    const float2 mcut2 = make_float2(-cut2, -cut2);
+    const int c = g.flat(ca, cb, cc);
+    int hs = start[c], he = start[c + 1];
+    for (int h0 = hs; h0 < he; h0 += 32) {
+        int i = h0 + lane;
+        bool own = i < he;
+        float4 xi = own ? posf[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        int n = 0;
+        int nrec = 0;  // chunk records waiting to be appended (warp-uniform)
+        // append the hits of the recorded chunks in order: one round per hit
+        // of this lane, a round that finds the current mask empty first moves
+        // on to the next record
+        auto flush = [&]() {
+            __syncwarp();
+            int k = 0;
+            unsigned m = sm.rec_mask[0][lane];
+            int4 meta = sm.rec_meta[0];
+            for (;;) {
+                while (m == 0 && ++k < nrec) {
+                    m = sm.rec_mask[k][lane];
+                    meta = sm.rec_meta[k];
+                }
+                if (m == 0) break;
+                int t = __clz(m);
+                m ^= 0x80000000u >> t;
+                int j = meta.x + t;
+                unsigned code = (unsigned)meta.y + (j >= meta.z ? 16u : 0u) + (j >= meta.w ? 16u : 0u);
+                append_entry(grp, n, cap, make_entry((unsigned)j, code), nbr4, N, i);
+            }
+            __syncwarp();
+            nrec = 0;
+        };
+        for (int a = -1; a <= 1; ++a) {
+            int na = ca + a, ia = na < 0 ? -1 : (na >= g.n[0] ? 1 : 0);
+            na -= ia * g.n[0];
+            for (int b = -1; b <= 1; ++b) {
+                int nb = cb + b, ib = nb < 0 ? -1 : (nb >= g.n[1] ? 1 : 0);
+                nb -= ib * g.n[1];
+                int col = g.flat(na, nb, 0);
+                // slot where the d = 0 and d = 1 cells of this column begin
+                int s0 = start[col + cc], s1 = start[col + (cc + 1 == nz ? 0 : cc + 1)];
+                float2 sx = make_float2(xi.x - ia * Lf.x, xi.x - ia * Lf.x);
+                float2 sy = make_float2(xi.y - ib * Lf.y, xi.y - ib * Lf.y);
+                for (int pc = 0; pc < npc; ++pc) {
+                    int zlo = cc + pd0[pc], zhi = cc + pd1[pc];
+                    zlo += zlo < 0 ? nz : (zlo >= nz ? -nz : 0);
+                    zhi += zhi < 0 ? nz : (zhi >= nz ? -nz : 0);
+                    int js = start[col + zlo], je = start[col + zhi + 1];
+                    float2 sz = make_float2(xi.z - pic[pc] * Lf.z, xi.z - pic[pc] * Lf.z);
+                    for (int j0 = js; j0 < je; j0 += 32) {
+                        int cntj = min(32, je - j0);
+                        __syncwarp();
+                        float4 q = lane < cntj ? posf[j0 + lane] : make_float4(1e18f, 1e18f, 1e18f, 0.f);
+                        sm.cxs[0][lane] = -q.x;
+                        sm.cxs[1][lane] = -q.y;
+                        sm.cxs[2][lane] = -q.z;
+                        __syncwarp();
+                        unsigned mask = 0;
+                        for (int t0 = 0; t0 < cntj; t0 += 8) {
+                            // r2 < cut2 exactly when r2 - cut2 is negative: its sign bit
+                            // is shifted into `sub`, first candidate highest
+                            unsigned sub = 0;
+#pragma unroll
+                            for (int t = 0; t < 8; t += 4) {
+                                float4 qx = *reinterpret_cast<const float4*>(&sm.cxs[0][t0 + t]);
+                                float4 qy = *reinterpret_cast<const float4*>(&sm.cxs[1][t0 + t]);
+                                float4 qz = *reinterpret_cast<const float4*>(&sm.cxs[2][t0 + t]);
+#pragma unroll
+                                for (int h = 0; h < 2; ++h) {
+                                    float2 px = h ? make_float2(qx.z, qx.w) : make_float2(qx.x, qx.y);
+                                    float2 py = h ? make_float2(qy.z, qy.w) : make_float2(qy.x, qy.y);
+                                    float2 pz = h ? make_float2(qz.z, qz.w) : make_float2(qz.x, qz.y);
+                                    float2 dx = __fadd2_rn(sx, px), dy = __fadd2_rn(sy, py), dz = __fadd2_rn(sz, pz);
+                                    float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+                                    float2 sg = __fadd2_rn(r2, mcut2);
+                                    sub = __funnelshift_l(__float_as_uint(sg.x), sub, 1);
+                                    sub = __funnelshift_l(__float_as_uint(sg.y), sub, 1);
+                                }
+                            }
+                            mask |= sub << (24 - t0);  // candidate t at bit 31 - t
+                        }
+                        if (cntj < 32) mask &= ~(0xffffffffu >> cntj);  // fillers past the range
+                        unsigned self = (unsigned)(i - j0);
+                        if (self < 32u) mask &= ~(0x80000000u >> self);
+                        if (!own) mask = 0;
+                        if (__any_sync(0xffffffffu, mask != 0u)) {
+                            sm.rec_mask[nrec][lane] = mask;
+                            if (lane == 0) {
+                                // the piece's z offsets: slot j lies in the cell
+                                // d = pd0 + (j >= s0 if the piece holds d = 0) + ...
+                                int dl = pd0[pc], dh = pd1[pc];
+                                sm.rec_meta[nrec] =
+                                    make_int4(j0, (int)offset_code(a, b, dl), dl < 0 && dh >= 0 ? s0 : INT_MAX,
+                                              dl < 1 && dh >= 1 ? s1 : INT_MAX);
+                            }
+                            if (++nrec == kBuildRecords) flush();
+                        }
+                    }
+                }
+            }
+        }
+        if (nrec) flush();
+        if (own) {
+            int m = n < cap ? n : cap;
+            cnt[i] = m;
+            if (m & 3) {  // pad the last group with the ghost slot
+                for (int k = m & 3; k < 4; ++k) grp[k] = make_entry((unsigned)N, kGhostCode);
+                nbr4[(size_t)(m >> 2) * N + i] = make_uint4(grp[0], grp[1], grp[2], grp[3]);
+            }
+            wmax = max(wmax, n);
+        }
+    }
+    return wmax;
+}
+
 static __global__ void __launch_bounds__(32 * kBuildWarps)
 build_list_warp_kernel(int N, const double4* __restrict__ pos, const float4* __restrict__ posf, Grid g,
                        const int* __restrict__ start, float3 Lf, float cut2, int cap,
                        uint4* __restrict__ nbr4, int* __restrict__ cnt, Scalars* sc, Gate gate) {
     if (!gate.open()) return;
-    __shared__ __align__(16) float cxs[kBuildWarps][3][32];
-    __shared__ unsigned grp_s[kBuildWarps][32][4];
-    __shared__ unsigned rec_mask[kBuildWarps][kBuildRecords][32];
-    // per chunk: first slot, entry code of its first cell, slots where the z
-    // offset of the code steps up by one (INT_MAX: none)
-    __shared__ int4 rec_meta[kBuildWarps][kBuildRecords];
+    __shared__ BuildSmem bs[kBuildWarps];
     int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int c = blockIdx.x * kBuildWarps + warp;
     int ncell = g.ncell();
     int wmax = 0;
-    unsigned (&grp)[4] = grp_s[warp][lane];
-    if (c < ncell) {
-        int ca = c / (g.n[1] * g.n[2]), cb = (c / g.n[2]) % g.n[1], cc = c % g.n[2];
-        int nz = g.n[2];
-        // the column's z cells d = -1, 0, 1 as at most two contiguous pieces,
-        // split where the column wraps (each piece has one z image)
-        int npc = 1, pd0[2] = {-1, 0}, pd1[2] = {1, 1}, pic[2] = {0, 0};
-        if (cc == 0) {
-            npc = 2; pd0[0] = -1; pd1[0] = -1; pic[0] = -1; pd0[1] = 0; pd1[1] = 1; pic[1] = 0;
-        } else if (cc == nz - 1) {
-            npc = 2; pd0[0] = -1; pd1[0] = 0; pic[0] = 0; pd0[1] = 1; pd1[1] = 1; pic[1] = 1;
-        }
-        const float2 mcut2 = make_float2(-cut2, -cut2);
-        int hs = start[c], he = start[c + 1];
-        for (int h0 = hs; h0 < he; h0 += 32) {
-            int i = h0 + lane;
-            bool own = i < he;
-            float4 xi = own ? posf[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-            int n = 0;
-            int nrec = 0;  // chunk records waiting to be appended (warp-uniform)
-            // append the hits of the recorded chunks in order: one round per hit
-            // of this lane, a round that finds the current mask empty first moves
-            // on to the next record
-            auto flush = [&]() {
-                __syncwarp();
-                int k = 0;
-                unsigned m = rec_mask[warp][0][lane];
-                int4 meta = rec_meta[warp][0];
-                for (;;) {
-                    while (m == 0 && ++k < nrec) {
-                        m = rec_mask[warp][k][lane];
-                        meta = rec_meta[warp][k];
-                    }
-                    if (m == 0) break;
-                    int t = __clz(m);
-                    m ^= 0x80000000u >> t;
-                    int j = meta.x + t;
-                    unsigned code = (unsigned)meta.y + (j >= meta.z ? 16u : 0u) + (j >= meta.w ? 16u : 0u);
-                    append_entry(grp, n, cap, make_entry((unsigned)j, code), nbr4, N, i);
-                }
-                __syncwarp();
-                nrec = 0;
-            };
-            for (int a = -1; a <= 1; ++a) {
-                int na = ca + a, ia = na < 0 ? -1 : (na >= g.n[0] ? 1 : 0);
-                na -= ia * g.n[0];
-                for (int b = -1; b <= 1; ++b) {
-                    int nb = cb + b, ib = nb < 0 ? -1 : (nb >= g.n[1] ? 1 : 0);
-                    nb -= ib * g.n[1];
-                    int col = g.flat(na, nb, 0);
-                    // slot where the d = 0 and d = 1 cells of this column begin
-                    int s0 = start[col + cc], s1 = start[col + (cc + 1 == nz ? 0 : cc + 1)];
-                    float2 sx = make_float2(xi.x - ia * Lf.x, xi.x - ia * Lf.x);
-                    float2 sy = make_float2(xi.y - ib * Lf.y, xi.y - ib * Lf.y);
-                    for (int pc = 0; pc < npc; ++pc) {
-                        int zlo = cc + pd0[pc], zhi = cc + pd1[pc];
-                        zlo += zlo < 0 ? nz : (zlo >= nz ? -nz : 0);
-                        zhi += zhi < 0 ? nz : (zhi >= nz ? -nz : 0);
-                        int js = start[col + zlo], je = start[col + zhi + 1];
-                        float2 sz = make_float2(xi.z - pic[pc] * Lf.z, xi.z - pic[pc] * Lf.z);
-                        for (int j0 = js; j0 < je; j0 += 32) {
-                            int cntj = min(32, je - j0);
-                            __syncwarp();
-                            float4 q = lane < cntj ? posf[j0 + lane] : make_float4(1e18f, 1e18f, 1e18f, 0.f);
-                            cxs[warp][0][lane] = -q.x;
-                            cxs[warp][1][lane] = -q.y;
-                            cxs[warp][2][lane] = -q.z;
-                            __syncwarp();
-                            unsigned mask = 0;
-                            for (int t0 = 0; t0 < cntj; t0 += 8) {
-                                // r2 < cut2 exactly when r2 - cut2 is negative: its sign bit
-                                // is shifted into `sub`, first candidate highest
-                                unsigned sub = 0;
-#pragma unroll
-                                for (int t = 0; t < 8; t += 4) {
-                                    float4 qx = *reinterpret_cast<const float4*>(&cxs[warp][0][t0 + t]);
-                                    float4 qy = *reinterpret_cast<const float4*>(&cxs[warp][1][t0 + t]);
-                                    float4 qz = *reinterpret_cast<const float4*>(&cxs[warp][2][t0 + t]);
-#pragma unroll
-                                    for (int h = 0; h < 2; ++h) {
-                                        float2 px = h ? make_float2(qx.z, qx.w) : make_float2(qx.x, qx.y);
-                                        float2 py = h ? make_float2(qy.z, qy.w) : make_float2(qy.x, qy.y);
-                                        float2 pz = h ? make_float2(qz.z, qz.w) : make_float2(qz.x, qz.y);
-                                        float2 dx = __fadd2_rn(sx, px), dy = __fadd2_rn(sy, py), dz = __fadd2_rn(sz, pz);
-                                        float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-                                        float2 sg = __fadd2_rn(r2, mcut2);
-                                        sub = __funnelshift_l(__float_as_uint(sg.x), sub, 1);
-                                        sub = __funnelshift_l(__float_as_uint(sg.y), sub, 1);
-                                    }
-                                }
-                                mask |= sub << (24 - t0);  // candidate t at bit 31 - t
-                            }
-                            if (cntj < 32) mask &= ~(0xffffffffu >> cntj);  // fillers past the range
-                            unsigned self = (unsigned)(i - j0);
-                            if (self < 32u) mask &= ~(0x80000000u >> self);
-                            if (!own) mask = 0;
-                            if (__any_sync(0xffffffffu, mask != 0u)) {
-                                rec_mask[warp][nrec][lane] = mask;
-                                if (lane == 0) {
-                                    // the piece's z offsets: slot j lies in the cell
-                                    // d = pd0 + (j >= s0 if the piece holds d = 0) + ...
-                                    int dl = pd0[pc], dh = pd1[pc];
-                                    rec_meta[warp][nrec] =
-                                        make_int4(j0, (int)offset_code(a, b, dl), dl < 0 && dh >= 0 ? s0 : INT_MAX,
-                                                  dl < 1 && dh >= 1 ? s1 : INT_MAX);
-                                }
-                                if (++nrec == kBuildRecords) flush();
-                            }
-                        }
-                    }
-                }
-            }
-            if (nrec) flush();
-            if (own) {
-                int m = n < cap ? n : cap;
-                cnt[i] = m;
-                if (m & 3) {  // pad the last group with the ghost slot
-                    for (int k = m & 3; k < 4; ++k) grp[k] = make_entry((unsigned)N, kGhostCode);
-                    nbr4[(size_t)(m >> 2) * N + i] = make_uint4(grp[0], grp[1], grp[2], grp[3]);
-                }
-                wmax = max(wmax, n);
-            }
-        }
-    }
+    if (c < ncell)
+        wmax = build_cell_lists(c / (g.n[1] * g.n[2]), (c / g.n[2]) % g.n[1], c % g.n[2], g, start, posf, Lf, cut2,
+                                cap, nbr4, cnt, N, bs[warp], lane);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) wmax = max(wmax, __shfl_down_sync(0xffffffffu, wmax, off));
     if (lane == 0 && c < ncell) {
