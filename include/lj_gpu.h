@@ -79,6 +79,11 @@ typedef struct lj_params {
      * tile whose window holds more reads from global memory). */
     int tile_cells;
     int tile_capacity;
+    /* Mixed path, neighbour-list kernel: 0 adds FP32 sums of 8 consecutive
+     * pair forces (and V, W) into the FP64 per-atom accumulators; 1 adds every
+     * pair's FP32 force, V and W in FP64 (no FP32 summation; slower).  Must be
+     * 0 with tile_cells > 0. */
+    int mixed_per_pair;
 } lj_params;
 
 /* One ThermodynamicMeasurement::Result (physics/measurements.hpp:42-56). */

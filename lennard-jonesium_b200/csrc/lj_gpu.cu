@@ -262,12 +262,15 @@ int launch_force_bs(lj_ctx* ctx, bool kick, const Fuse& fz) {
     }
     if (ctx->p.precision == LJ_PRECISION_MIXED && kind == LJ_FORCE_LJ && !ctx->small_box) {
         MixedParams mp = mixed_params(ctx->pp, ctx->list_grid);
-        if (kick)
-            force_mixed_kernel<true, BS><<<gr, bl, 0, ctx->stream>>>(N, ctx->posl, s, ctx->nbr, ctx->cnt, ctx->pp, mp,
-                                                                     ctx->partials, fz);
-        else
-            force_mixed_kernel<false, BS><<<gr, bl, 0, ctx->stream>>>(N, ctx->posl, s, ctx->nbr, ctx->cnt, ctx->pp, mp,
-                                                                      ctx->partials, fz);
+#define LJ_MIXED_LAUNCH(KK, PP)                                                                          \
+    force_mixed_kernel<KK, BS, PP><<<gr, bl, 0, ctx->stream>>>(N, ctx->posl, s, ctx->nbr, ctx->cnt, ctx->pp, mp, \
+                                                               ctx->partials, fz)
+        if (ctx->p.mixed_per_pair) {
+            if (kick) LJ_MIXED_LAUNCH(true, true); else LJ_MIXED_LAUNCH(false, true);
+        } else {
+            if (kick) LJ_MIXED_LAUNCH(true, false); else LJ_MIXED_LAUNCH(false, false);
+        }
+#undef LJ_MIXED_LAUNCH
         CKL();
         return LJ_OK;
     }
@@ -753,6 +756,9 @@ int lj_gpu_create(const lj_params* params, lj_ctx** out) {
     if (p.force_kind < LJ_FORCE_NONE || p.force_kind > LJ_FORCE_CONSTANT) return LJ_ERR_ARG;
     if (p.precision != LJ_PRECISION_FP64 && p.precision != LJ_PRECISION_MIXED) return LJ_ERR_ARG;
     if (!p.periodic && p.force_kind != LJ_FORCE_NONE) return LJ_ERR_ARG;
+    // per-pair FP64 sums exist for the neighbour-list mixed kernel, not the tiles
+    if (p.mixed_per_pair != 0 && p.mixed_per_pair != 1) return LJ_ERR_ARG;
+    if (p.mixed_per_pair && p.tile_cells > 0) return LJ_ERR_ARG;
     // lennard_jones_force.cpp:45 -- the cutoff must lie beyond the potential minimum
     if (p.force_kind == LJ_FORCE_LJ && !(p.cutoff_distance * p.cutoff_distance > std::cbrt(2.0)))
         return LJ_ERR_ARG;
@@ -1124,7 +1130,8 @@ extern "C" {
 // parameters.  Candidates: the Verlet skin, which sets the list-cell edge
 // rc + skin and, against it, the rebuild frequency; and per skin either the
 // pair kernel's block size (atoms per block: 64, 128, 256) and, on the mixed
-// path, also its shared-memory tile variant at 3 or 6 cells per tile.
+// path (chunked FP32 pair sums), also its shared-memory tile variant at 3 or
+// 6 cells per tile.
 // Each candidate runs in its own context from the same initial state after a
 // warm-up long enough to build the step graph and the first neighbour list.
 int lj_gpu_autotune(const lj_params* base, const double* x, const double* v, int stride, int steps,
@@ -1143,7 +1150,7 @@ int lj_gpu_autotune(const lj_params* base, const double* x, const double* v, int
         last_skin = eff;
         Grid lg = make_grid(base->box, base->cutoff_distance + eff);
         bool tiled = base->precision == LJ_PRECISION_MIXED && base->force_kind == LJ_FORCE_LJ &&
-                     std::min(lg.n[0], std::min(lg.n[1], lg.n[2])) >= 3;
+                     !base->mixed_per_pair && std::min(lg.n[0], std::min(lg.n[1], lg.n[2])) >= 3;
         for (int q = 0; q < (tiled ? 5 : 3); ++q) {
             lj_params p = *base;
             p.skin = sk;

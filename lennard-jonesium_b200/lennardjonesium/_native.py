@@ -32,6 +32,7 @@ class Params(ctypes.Structure):
         ("force_block", ctypes.c_int),
         ("tile_cells", ctypes.c_int),
         ("tile_capacity", ctypes.c_int),
+        ("mixed_per_pair", ctypes.c_int),
     ]
 
 

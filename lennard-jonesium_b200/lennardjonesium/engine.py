@@ -60,11 +60,12 @@ def autotune(N, box, x, v, steps=100, **kw):
     xs, vs = _as4(x, N), _as4(v, N) if v is not None else None
     nat.check(nat.lib().lj_gpu_autotune(ctypes.byref(base), _p(xs), _p(vs), 4, int(steps), ctypes.byref(best),
                                         ctypes.byref(ms)))
-    return {"skin": best.skin, "force_block": best.force_block, "tile_cells": best.tile_cells}, ms.value
+    return {"skin": best.skin, "force_block": best.force_block, "tile_cells": best.tile_cells,
+            "mixed_per_pair": bool(best.mixed_per_pair)}, ms.value
 
 
 def _params(N, box, cutoff=2.5, dt=0.005, precision="fp64", force="lj", strength=0.0, periodic=True, device=0,
-            skin=None, capacity=0, force_block=0, tile_cells=0, tile_capacity=0):
+            skin=None, capacity=0, force_block=0, tile_cells=0, tile_capacity=0, mixed_per_pair=False):
     L = nat.lib()
     p = nat.Params()
     L.lj_gpu_default_params(ctypes.byref(p))
@@ -84,6 +85,7 @@ def _params(N, box, cutoff=2.5, dt=0.005, precision="fp64", force="lj", strength
     p.force_block = int(force_block)
     p.tile_cells = int(tile_cells)
     p.tile_capacity = int(tile_capacity)
+    p.mixed_per_pair = 1 if mixed_per_pair else 0
     return p
 
 
@@ -91,11 +93,12 @@ class GpuSystem:
     """One periodic LJ system resident on a GPU."""
 
     def __init__(self, N, box, cutoff=2.5, dt=0.005, precision="fp64", force="lj", strength=0.0,
-                 periodic=True, device=0, skin=None, capacity=0, force_block=0, tile_cells=0, tile_capacity=0):
+                 periodic=True, device=0, skin=None, capacity=0, force_block=0, tile_cells=0, tile_capacity=0,
+                 mixed_per_pair=False):
         L = nat.lib()
         p = _params(N, box, cutoff=cutoff, dt=dt, precision=precision, force=force, strength=strength,
                     periodic=periodic, device=device, skin=skin, capacity=capacity, force_block=force_block,
-                    tile_cells=tile_cells, tile_capacity=tile_capacity)
+                    tile_cells=tile_cells, tile_capacity=tile_capacity, mixed_per_pair=mixed_per_pair)
         b = np.broadcast_to(np.asarray(box, dtype=np.float64), (3,))
         self.N = int(N)
         self.box = b.copy()

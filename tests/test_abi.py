@@ -65,6 +65,11 @@ def test_create_rejects_bad_arguments():
     p.cutoff_distance = 2.5
     p.periodic = 0  # forces without the periodic boundary are not a reference configuration
     assert L.lj_gpu_create(ctypes.byref(p), ctypes.byref(ctx)) == _native.LJ_ERR_ARG
+    p.periodic = 1
+    p.mixed_per_pair = 2  # a flag: 0 or 1
+    assert L.lj_gpu_create(ctypes.byref(p), ctypes.byref(ctx)) == _native.LJ_ERR_ARG
+    p.mixed_per_pair, p.tile_cells = 1, 3  # per-pair FP64 sums are not built for the tiles
+    assert L.lj_gpu_create(ctypes.byref(p), ctypes.byref(ctx)) == _native.LJ_ERR_ARG
 
 
 def test_host_initial_condition_matches_oracle():

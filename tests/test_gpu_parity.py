@@ -285,14 +285,16 @@ def test_rdf_bit_exact(N, rho, rmax):
     assert np.array_equal(h, ljref.rdf(x, L, 200, rmax))
 
 
-def test_mixed_precision_force_error():
-    """Mixed path (FP32 pair arithmetic) vs FP64: stated bounds."""
+@pytest.mark.parametrize("per_pair", [False, True])
+def test_mixed_precision_force_error(per_pair):
+    """Mixed path (FP32 pair arithmetic) vs FP64: stated bounds, with 8-pair FP32
+    sums into the FP64 accumulators and with every pair added in FP64."""
     x, v, L = perturbed_fcc(4000, 1.2, 0.8, 7)
     with gpu_system(4000, L) as g:
         g.upload(x)
         pe64, w64 = g.compute_forces()
         F64 = g.download()["F"]
-    with gpu_system(4000, L, precision="mixed") as g:
+    with gpu_system(4000, L, precision="mixed", mixed_per_pair=per_pair) as g:
         g.upload(x)
         pe32, w32 = g.compute_forces()
         F32 = g.download()["F"]
