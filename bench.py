@@ -60,7 +60,8 @@ def measured_peaks():
 
 
 def alg_flops_per_atom_step(N, L, rc, rho):
-    """Survey-defined algorithmic work of the reference's half-shell algorithm:
+    """Algorithmic work of the reference's half-shell algorithm (candidate tests
+    of the 27-cell stencil counted once per pair, kept pairs likewise):
     F = 9 C + 30 P, C = (27 rho a^3 - 1) / 2 candidate tests, P = (2 pi / 3) rho rc^3 pairs."""
     n_c = math.floor(L / rc)
     a = L / n_c
