@@ -336,7 +336,8 @@ build_list_kernel(int N, const double4* __restrict__ pos, const float4* __restri
 // instead of the busiest lane's hits in every chunk added up.  Each lane
 // collects entries in a 4-entry shared buffer and writes whole groups (one
 // 16-byte store).  Entries, their order (stencil cell, then slot) and the
-// candidate radius are those of build_list_kernel<false>.
+// candidate radius are those of build_list_kernel<false>.  The per-cell body,
+// build_cell_lists, also serves the batched engine's list build.
 constexpr int kBuildWarps = 4;
 constexpr int kBuildRecords = 24;
 
