@@ -82,3 +82,44 @@ def test_host_initial_condition_matches_oracle():
         assert L == Lo
         assert np.array_equal(x, xo)
         assert np.allclose(v, vo, rtol=0, atol=1e-14)
+
+
+def _header_struct(name):
+    """(type, field) pairs of `typedef struct name {...} name;` in include/lj_gpu.h, in order."""
+    text = re.sub(r"/\*.*?\*/", "", (ROOT / "include" / "lj_gpu.h").read_text(), flags=re.S)
+    body = re.search(r"typedef struct %s \{(.*?)\} %s;" % (name, name), text, flags=re.S).group(1)
+    out = []
+    for decl in body.split(";"):
+        decl = " ".join(decl.split())
+        if not decl:
+            continue
+        m = re.match(r"(unsigned long long|long long|double|int|unsigned)\s+(.*)", decl)
+        assert m, decl
+        for field in m.group(2).split(","):
+            out.append((m.group(1), field.strip()))
+    return out
+
+
+_CTYPES = {"int": ctypes.c_int, "double": ctypes.c_double, "long long": ctypes.c_longlong}
+
+
+@pytest.mark.parametrize("name,cls", [("lj_params", "Params"), ("lj_stats", "Stats")])
+def test_ctypes_structs_follow_the_header(name, cls):
+    """The Python binding's structs list the header's fields in the header's order and types."""
+    from lennardjonesium import _native
+    fields = getattr(_native, cls)._fields_
+    decl = _header_struct(name)
+    assert len(fields) == len(decl)
+    for (fname, ftype), (ctype, cdecl) in zip(fields, decl):
+        m = re.match(r"(\w+)(?:\[(\d+)\])?$", cdecl)
+        assert fname == m.group(1)
+        base = _CTYPES[ctype]
+        assert ftype == (base * int(m.group(2)) if m.group(2) else base)
+
+
+def test_integration_cython_params_follow_the_header():
+    """The Cython declaration shown for maintainers lists lj_params' fields in order."""
+    text = (ROOT / "INTEGRATION.md").read_text()
+    block = re.search(r"ctypedef struct lj_params:\n((?:        .*\n)+)", text).group(1)
+    shown = [" ".join(line.split()) for line in block.splitlines()]
+    assert shown == [f"{t} {f}" for t, f in _header_struct("lj_params")]
