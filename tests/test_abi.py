@@ -93,17 +93,21 @@ def _header_struct(name):
         decl = " ".join(decl.split())
         if not decl:
             continue
-        m = re.match(r"(unsigned long long|long long|double|int|unsigned)\s+(.*)", decl)
+        m = re.match(r"(const char\*|unsigned long long|long long|double|int|unsigned)\s*(.*)", decl)
         assert m, decl
         for field in m.group(2).split(","):
             out.append((m.group(1), field.strip()))
     return out
 
 
-_CTYPES = {"int": ctypes.c_int, "double": ctypes.c_double, "long long": ctypes.c_longlong}
+_CTYPES = {"int": ctypes.c_int, "double": ctypes.c_double, "long long": ctypes.c_longlong,
+           "unsigned": ctypes.c_uint, "const char*": ctypes.c_char_p}
 
 
-@pytest.mark.parametrize("name,cls", [("lj_params", "Params"), ("lj_stats", "Stats")])
+@pytest.mark.parametrize("name,cls", [("lj_params", "Params"), ("lj_stats", "Stats"), ("lj_thermo", "Thermo"),
+                                      ("lj_phase_times", "PhaseTimes"), ("lj_sim_config", "SimConfig"),
+                                      ("lj_sim_result", "SimResult"), ("lj_batch_system", "BatchSystem"),
+                                      ("lj_adj_params", "AdjParams")])
 def test_ctypes_structs_follow_the_header(name, cls):
     """The Python binding's structs list the header's fields in the header's order and types."""
     from lennardjonesium import _native
