@@ -127,3 +127,45 @@ def test_integration_cython_params_follow_the_header():
     block = re.search(r"ctypedef struct lj_params:\n((?:        .*\n)+)", text).group(1)
     shown = [" ".join(line.split()) for line in block.splitlines()]
     assert shown == [f"{t} {f}" for t, f in _header_struct("lj_params")]
+
+
+def _prototypes():
+    """name -> (return type, [parameter types]) of the functions include/lj_gpu.h declares."""
+    text = re.sub(r"/\*.*?\*/", "", (ROOT / "include" / "lj_gpu.h").read_text(), flags=re.S)
+    text = re.sub(r"//[^\n]*", "", text)
+    out = {}
+    for m in re.finditer(r"([A-Za-z_][\w\s\*]*?)\b(lj_\w+)\s*\(([^)]*)\)\s*;", text):
+        ret = " ".join(m.group(1).split())
+        params = [" ".join(p.split()) for p in m.group(3).split(",") if p.strip() and p.strip() != "void"]
+        out[m.group(2)] = (ret, params)
+    return out
+
+
+def _kind(decl):
+    """ctypes class a C parameter or return type maps to (pointers as c_void_p)."""
+    decl = re.sub(r"\b(const|struct)\b", "", decl)
+    if "*" in decl:
+        return "char_p" if re.match(r"\s*char\s*\*\s*\w*$", decl) else "ptr"
+    words = decl.split()
+    base = " ".join(w for w in words[:-1]) if len(words) > 1 else words[0]
+    return {"int": "int", "double": "double", "long long": "longlong", "void": "void",
+            "unsigned": "uint", "unsigned long long": "ulonglong"}[base]
+
+
+def test_signatures_follow_the_header():
+    """Return and parameter types of every binding agree with the header's prototypes."""
+    from lennardjonesium import _native
+    as_kind = {None: "void", ctypes.c_int: "int", ctypes.c_double: "double", ctypes.c_longlong: "longlong",
+               ctypes.c_uint: "uint", ctypes.c_ulonglong: "ulonglong", ctypes.c_char_p: "char_p",
+               ctypes.c_void_p: "ptr"}
+    protos = _prototypes()
+    for name, (res, args) in _native.SIGNATURES.items():
+        ret, params = protos[name]
+        want_ret = "ptr" if "*" in ret else _kind(ret + " x")
+        if want_ret == "ptr" and res is ctypes.c_char_p:
+            want_ret = "char_p"
+        assert as_kind[res] == want_ret, name
+        assert len(args) == len(params), name
+        for a, prm in zip(args, params):
+            k = _kind(prm)
+            assert as_kind[a] == k or (k == "char_p" and as_kind[a] == "ptr"), (name, prm)
