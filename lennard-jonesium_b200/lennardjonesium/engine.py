@@ -90,7 +90,17 @@ def _params(N, box, cutoff=2.5, dt=0.005, precision="fp64", force="lj", strength
 
 
 class GpuSystem:
-    """One periodic LJ system resident on a GPU."""
+    """One periodic LJ system resident on a GPU (a context of include/lj_gpu.h).
+
+    N, box: atom count and box edge (a scalar or three edges); cutoff, dt: rc
+    and the time step.  precision: "fp64" (the drop-in path) or "mixed" (FP32
+    pair arithmetic, FP64 accumulation and integration).  force: "lj", "constant"
+    (the reference's test mock, with `strength`) or "none".  skin: Verlet skin
+    (None: 0.3); capacity: list entries per atom (0: density-based);
+    force_block: atoms per pair-kernel block (64, 128, 256; 0: 128).  Mixed path
+    only: tile_cells / tile_capacity select the shared-memory tile kernel, and
+    mixed_per_pair adds every pair force in FP64 instead of FP32 sums of 8
+    pairs.  Every call raises LJError on a non-zero status."""
 
     def __init__(self, N, box, cutoff=2.5, dt=0.005, precision="fp64", force="lj", strength=0.0,
                  periodic=True, device=0, skin=None, capacity=0, force_block=0, tile_cells=0, tile_capacity=0,
