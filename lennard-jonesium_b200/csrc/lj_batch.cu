@@ -239,7 +239,9 @@ b_copy_back_kernel(const int* __restrict__ sys_of, const SysState* st, int Ntot,
 
 // Warp-per-cell list build: the per-cell body of build_list_warp_kernel, on
 // the grid and slot ranges of the cell's own system (entries identical to a
-// single-system build of that system).
+// single-system build of that system).  Six resident blocks leave it up to 80
+// registers, where it does not spill (the per-system indexing costs the
+// registers the single-system kernel fits into 64).
 static __global__ void __launch_bounds__(32 * kBuildWarps, 6)
 b_build_list_kernel(const int* __restrict__ cell_sys, const SysDev* __restrict__ sys, SysState* st, int ncell_tot,
                     int Ntot, const float4* __restrict__ posf, const int* __restrict__ start, int cap,
