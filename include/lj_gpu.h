@@ -177,6 +177,19 @@ long long lj_gpu_debug_pairs(lj_ctx* ctx, long long cap, int* i, int* j, int* im
  * has no RDF.) */
 int lj_gpu_rdf(lj_ctx* ctx, int nbins, double rmax, unsigned long long* hist);
 
+/* The RDF sampled along a run without host round trips (new, like lj_gpu_rdf):
+ * lj_gpu_rdf_accumulate enqueues one sample of the current positions on the
+ * context's stream, adding its counts to a device-resident histogram, and
+ * returns without waiting; the cell-list scratch is allocated on the first
+ * sample and kept, so later samples allocate nothing.  Every sample of one
+ * accumulation must use the same nbins and rmax (LJ_ERR_ARG otherwise).
+ * lj_gpu_rdf_read waits for the stream and copies the summed counts (nbins of
+ * the accumulation; hist may be NULL) and the number of samples (may be NULL).
+ * lj_gpu_rdf_reset starts a new accumulation. */
+int lj_gpu_rdf_accumulate(lj_ctx* ctx, int nbins, double rmax);
+int lj_gpu_rdf_read(lj_ctx* ctx, unsigned long long* hist, long long* samples);
+int lj_gpu_rdf_reset(lj_ctx* ctx);
+
 int lj_gpu_get_stats(const lj_ctx* ctx, lj_stats* out);
 
 /* The context's CUDA stream (a cudaStream_t), for callers that time or order
@@ -190,10 +203,13 @@ int lj_gpu_step_async(lj_ctx* ctx, int nsteps);
 int lj_gpu_synchronize(lj_ctx* ctx);
 
 /* Device time of each phase of the step, accumulated over nsteps real steps
- * with CUDA events recorded between the phases on the context's stream. */
+ * with CUDA events recorded between the phases on the context's stream.  The
+ * host reads the rebuild criterion after each kick/drift (one synchronisation
+ * per step) and launches the rebuild chain only when it holds. */
 typedef struct lj_phase_times {
     double kick_drift_ms;  /* first half kick, drift, wrap, displacement check */
-    double rebuild_ms;     /* cell binning + neighbour list (mostly gated off) */
+    double rebuild_ms;     /* cell binning + neighbour list, launched only on the steps whose
+                              rebuild criterion holds (as in the step graphs) */
     double force_ms;       /* pair force + second kick + partial sums */
     double finalize_ms;    /* fixed-order reduction and record */
     long long steps;
@@ -225,14 +241,19 @@ int lj_gpu_fma_peaks(int device, double* fp64_tflops, double* fp32_tflops);
  *   hist  device, nbins unsigned 64-bit counts (overwritten)
  *   box   host, 3 edge lengths; rmax <= min(box) / 2
  *   stream  cudaStream_t to run on (NULL: the legacy default stream)
+ *   pos must be 16-byte aligned and hist 8-byte aligned (LJ_ERR_ARG otherwise).
  * The work is enqueued on the stream and the call returns without waiting.
- * Counts are those of lj_gpu_rdf.  Limits: N <= 131072, nbins <= 12288, and at
- * most 32768 cells of edge >= rmax; larger inputs return LJ_ERR_ARG.
+ * Counts are those of lj_gpu_rdf.  Limits: N <= 131072 and nbins <= 12288;
+ * larger inputs return LJ_ERR_ARG.  The cell list has at most 32768 cells:
+ * a box that holds more cells of edge rmax gets coarser cells (same counts,
+ * more candidate pairs).
  *
  * Scratch is one fixed device array inside this library (about 5.3 MB, held on
  * every GPU that loads the library until the process exits).  The first call
- * on a device looks up that array's device address (cudaGetSymbolAddress), so
- * make the first call on each device before any stream capture.  Calls share
+ * on a device looks up that array's device address (cudaGetSymbolAddress) and
+ * caches it, so make the first call on each device before any stream capture;
+ * a device reset (cudaDeviceReset) may move the array and invalidates the
+ * cached address, so do not call this after resetting a device.  Calls share
  * the array: calls whose GPU work overlaps (other streams, other threads) race
  * and must be serialised by the caller. */
 int lj_gpu_rdf_noalloc(const double* pos, int N, const double* box, int nbins, double rmax,

@@ -95,6 +95,8 @@ struct lj_ctx {
     int* dbg_members = nullptr;
     int* dbg_cell_of = nullptr;
     int* dbg_tiles = nullptr;
+    // RDF cell-list scratch and device accumulator, sized on first use
+    RdfScratch rdf{};
 
     long long launches = 0;       // kernels launched directly (gated-off ones included)
     long long host_steps = 0;     // mirror of the device step counter
@@ -562,6 +564,7 @@ void free_all(lj_ctx* c) {
                     c->dbg_members, c->dbg_cell_of, c->dbg_tiles};
     for (void* q : ptrs)
         if (q) cudaFree(q);
+    rdf_release(c->rdf);
     if (c->host_ring) cudaFreeHost(c->host_ring);
     for (StepGraph& g : c->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -712,6 +715,21 @@ int init_ctx(lj_ctx* ctx, const lj_params& p) {
     int one = 1;
     CK(cudaMemcpyAsync(&ctx->sc->need_rebuild, &one, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    return LJ_OK;
+}
+
+// Argument checks, grid and scratch of one RDF sample (allocates only when
+// the scratch must grow: the first sample, or a larger nbins).
+int rdf_prepare(lj_ctx* ctx, int nbins, double rmax, Grid& g) {
+    if (nbins < 1 || !(rmax > 0)) return set_err(ctx, LJ_ERR_ARG, "bad rdf arguments");
+    if ((size_t)nbins * sizeof(unsigned) > 200 * 1024)
+        return set_err(ctx, LJ_ERR_ARG, "rdf: too many bins for the shared-memory histogram");
+    for (int k = 0; k < 3; ++k)
+        if (rmax > 0.5 * ctx->pp.L[k]) return set_err(ctx, LJ_ERR_ARG, "rmax exceeds half the box");
+    CK(cudaSetDevice(ctx->p.device));
+    g = rdf_grid(ctx->pp.L, rmax, (long long)kScanTile * kMaxScanTiles);
+    if (rdf_reserve(ctx->rdf, ctx->N, rdf_uses_cells(g) ? g.ncell() : 1, nbins) || rdf_set_smem(nbins))
+        return set_err(ctx, LJ_ERR_CUDA, "rdf: scratch allocation failed");
     return LJ_OK;
 }
 
@@ -1051,11 +1069,59 @@ int lj_gpu_get_stats(const lj_ctx* ctx_c, lj_stats* out) {
 }
 
 int lj_gpu_rdf(lj_ctx* ctx, int nbins, double rmax, unsigned long long* hist) {
-    if (!ctx || nbins < 1 || !hist || !(rmax > 0)) return set_err(ctx, LJ_ERR_ARG, "bad rdf arguments");
-    for (int k = 0; k < 3; ++k)
-        if (rmax > 0.5 * ctx->pp.L[k]) return set_err(ctx, LJ_ERR_ARG, "rmax exceeds half the box");
-    return rdf_launch(ctx->N, ctx->pos, ctx->pp, nbins, rmax, hist, ctx->stream, ctx->err, sizeof ctx->err,
-                      &ctx->launches);
+    if (!ctx || !hist) return set_err(ctx, LJ_ERR_ARG, "bad rdf arguments");
+    Grid g{};
+    int rc = rdf_prepare(ctx, nbins, rmax, g);
+    if (rc) return rc;
+    // a single sample goes to the second half of the scratch histogram, so a
+    // running accumulation is left alone
+    unsigned long long* once = ctx->rdf.hist + ctx->rdf.bins;
+    CK(cudaMemsetAsync(once, 0, sizeof(unsigned long long) * nbins, ctx->stream));
+    if (rdf_enqueue(ctx->N, ctx->pos, ctx->pp, g, nbins, rmax, ctx->rdf, once, ctx->stream, &ctx->launches))
+        return set_err(ctx, LJ_ERR_CUDA, "rdf: kernel launch failed");
+    CK(cudaMemcpyAsync(hist, once, sizeof(unsigned long long) * nbins, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return LJ_OK;
+}
+
+int lj_gpu_rdf_accumulate(lj_ctx* ctx, int nbins, double rmax) {
+    if (!ctx) return LJ_ERR_ARG;
+    RdfScratch& r = ctx->rdf;
+    if (r.samples > 0 && (nbins != r.acc_bins || rmax != r.acc_rmax))
+        return set_err(ctx, LJ_ERR_ARG, "rdf_accumulate: nbins and rmax differ from the running accumulation");
+    Grid g{};
+    int rc = rdf_prepare(ctx, nbins, rmax, g);
+    if (rc) return rc;
+    if (r.samples == 0) {
+        CK(cudaMemsetAsync(r.hist, 0, sizeof(unsigned long long) * nbins, ctx->stream));
+        r.acc_bins = nbins;
+        r.acc_rmax = rmax;
+    }
+    if (rdf_enqueue(ctx->N, ctx->pos, ctx->pp, g, nbins, rmax, r, r.hist, ctx->stream, &ctx->launches))
+        return set_err(ctx, LJ_ERR_CUDA, "rdf: kernel launch failed");
+    ++r.samples;
+    return LJ_OK;
+}
+
+int lj_gpu_rdf_read(lj_ctx* ctx, unsigned long long* hist, long long* samples) {
+    if (!ctx) return LJ_ERR_ARG;
+    CK(cudaSetDevice(ctx->p.device));
+    const RdfScratch& r = ctx->rdf;
+    if (samples) *samples = r.samples;
+    if (hist && r.samples > 0) {
+        CK(cudaMemcpyAsync(hist, r.hist, sizeof(unsigned long long) * r.acc_bins, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    return LJ_OK;
+}
+
+int lj_gpu_rdf_reset(lj_ctx* ctx) {
+    if (!ctx) return LJ_ERR_ARG;
+    ctx->rdf.samples = 0;
+    ctx->rdf.acc_bins = 0;
+    ctx->rdf.acc_rmax = 0.0;
+    return LJ_OK;
 }
 
 }  // extern "C"
@@ -1085,12 +1151,24 @@ int lj_gpu_step_timed(lj_ctx* ctx, int nsteps, lj_phase_times* out) {
     Scalars before;
     CK(cudaMemcpy(&before, ctx->sc, sizeof before, cudaMemcpyDeviceToHost));
     bool forces = ctx->p.force_kind != LJ_FORCE_NONE;
+    const Gate gate = gate_of(ctx);
     for (int s = 0; s < nsteps; ++s) {
         int rc;
         CK(cudaEventRecord(ev[0], ctx->stream));
         if ((rc = launch_kick_drift(ctx))) return rc;
         CK(cudaEventRecord(ev[1], ctx->stream));
-        if (forces && (rc = launch_rebuild(ctx))) return rc;
+        if (forces) {
+            // launch the rebuild chain only on the steps whose gate is open, as
+            // the step graphs' conditional node does (the host reads the
+            // criterion kick_drift just computed)
+            Scalars h;
+            CK(cudaMemcpyAsync(&h, ctx->sc, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            double d2;
+            std::memcpy(&d2, &h.max_disp2, sizeof d2);
+            bool open = gate.always || h.need_rebuild || d2 > gate.thresh2;
+            if (open && (rc = launch_rebuild(ctx))) return rc;
+        }
         CK(cudaEventRecord(ev[2], ctx->stream));
         if (forces) {
             if ((rc = launch_force(ctx, true))) return rc;

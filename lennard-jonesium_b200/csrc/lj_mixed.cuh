@@ -187,8 +187,38 @@ force_mixed_kernel(int N, const float4* __restrict__ posl, Soa s, const uint4* _
 }
 
 // Radial distribution histogram (lj_rdf.cu).
-int rdf_launch(int N, const double4* pos, const PairParams& pp, int nbins, double rmax,
-               unsigned long long* hist_host, cudaStream_t stream, char* err, size_t errlen,
-               long long* launches);
+//
+// Scratch of the cell-list histogram: sized on first use and kept, so that a
+// sample costs no allocation and no synchronisation.  hist holds two
+// histograms of `bins` counts: the running accumulator, then a single sample.
+struct RdfScratch {
+    int atoms = 0, cells = 0, bins = 0;  // capacities
+    int* cell_of = nullptr;
+    int* rank = nullptr;
+    int* count = nullptr;
+    int* start = nullptr;
+    int* tiles = nullptr;
+    double4* sorted = nullptr;
+    unsigned long long* hist = nullptr;
+    // the running accumulation (lj_gpu_rdf_accumulate)
+    int acc_bins = 0;
+    double acc_rmax = 0.0;
+    long long samples = 0;
+};
+
+// Grid of cells of edge >= rmax with at most max_cells cells (coarser cells
+// where the box holds more; the histogram does not depend on the cell size).
+Grid rdf_grid(const double L[3], double rmax, long long max_cells);
+// The cell-list kernels need >= 3 cells per axis; otherwise all pairs.
+bool rdf_uses_cells(const Grid& g);
+// Grow the scratch to N atoms, ncell cells and nbins bins (returns 2 on a CUDA error).
+int rdf_reserve(RdfScratch& s, int N, int ncell, int nbins);
+void rdf_release(RdfScratch& s);
+// Allow a shared-memory histogram of nbins counts (above 48 KB).
+int rdf_set_smem(int nbins);
+// Enqueue one sample: ordered pairs counted into hist (device, nbins counts),
+// which is added to, not cleared.  Returns 0, or 2 on a CUDA error.
+int rdf_enqueue(int N, const double4* pos, const PairParams& pp, const Grid& g, int nbins, double rmax,
+                const RdfScratch& s, unsigned long long* hist, cudaStream_t stream, long long* launches);
 
 }  // namespace ljb

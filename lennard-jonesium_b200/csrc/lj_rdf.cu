@@ -11,7 +11,9 @@
 // boxes use all pairs.  Each block accumulates a shared-memory
 // histogram and adds it to the global 64-bit histogram once.
 
+#include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 
@@ -109,77 +111,113 @@ __global__ void rdf_place_kernel(int N, const double4* __restrict__ pos, const i
 
 }  // namespace
 
-int rdf_launch(int N, const double4* pos, const PairParams& pp, int nbins, double rmax,
-               unsigned long long* hist_host, cudaStream_t stream, char* err, size_t errlen,
-               long long* launches) {
-    if ((size_t)nbins * sizeof(unsigned) > 200 * 1024) {
-        std::snprintf(err, errlen, "rdf: too many bins for the shared-memory histogram");
-        return 1;  // LJ_ERR_ARG
-    }
-    Grid g;
-    int nmin = 1 << 30;
-    for (int k = 0; k < 3; ++k) {
-        g.n[k] = (int)floor(pp.L[k] / rmax);
-        if (g.n[k] < 1) g.n[k] = 1;
-        g.ratio[k] = (double)g.n[k] / pp.L[k];
-        nmin = g.n[k] < nmin ? g.n[k] : nmin;
-    }
-    bool cells = nmin >= 3 && g.ncell() <= kScanTile * kMaxScanTiles;
-    unsigned long long* dh = nullptr;
-    int *cell_of = nullptr, *rank = nullptr, *count = nullptr, *start = nullptr, *tiles = nullptr;
-    double4* sorted = nullptr;
-    cudaError_t e = cudaMalloc(&dh, sizeof(unsigned long long) * nbins);
-    size_t shm = sizeof(unsigned) * nbins;
-    if (e == cudaSuccess) e = cudaMemsetAsync(dh, 0, sizeof(unsigned long long) * nbins, stream);
-    if (e == cudaSuccess && shm > 48 * 1024) {
-        e = cudaFuncSetAttribute(rdf_cells_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(rdf_all_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-    }
-    double rmax2 = rmax * rmax, inv_dr = (double)nbins / rmax;
-    int blocks = (N + kThreads - 1) / kThreads;
-    if (e == cudaSuccess && !cells) {
-        rdf_all_pairs_kernel<<<blocks, kThreads, shm, stream>>>(N, pos, pp, rmax2, inv_dr, nbins, dh);
-        e = cudaGetLastError();
-        ++*launches;
-    } else if (e == cudaSuccess) {
-        int nc = g.ncell();
-        int ntiles = (nc + kScanTile - 1) / kScanTile;
-        e = cudaMalloc(&cell_of, sizeof(int) * N);
-        if (e == cudaSuccess) e = cudaMalloc(&rank, sizeof(int) * N);
-        if (e == cudaSuccess) e = cudaMalloc(&count, sizeof(int) * nc);
-        if (e == cudaSuccess) e = cudaMalloc(&start, sizeof(int) * (nc + 1));
-        if (e == cudaSuccess) e = cudaMalloc(&tiles, sizeof(int) * kMaxScanTiles);
-        if (e == cudaSuccess) e = cudaMalloc(&sorted, sizeof(double4) * N);
-        if (e == cudaSuccess) e = cudaMemsetAsync(count, 0, sizeof(int) * nc, stream);
-        if (e == cudaSuccess) {
-            Gate open{};
-            open.always = 1;
-            rdf_bin_kernel<<<blocks, kThreads, 0, stream>>>(N, pos, g, cell_of, rank, count);
-            scan_reduce_kernel<false><<<ntiles, 1024, 0, stream>>>(count, nc, tiles, open);
-            scan_tiles_kernel<false><<<1, 1024, 0, stream>>>(tiles, ntiles, open);
-            scan_apply_kernel<false><<<ntiles, 1024, 0, stream>>>(count, nc, tiles, start, open);
-            rdf_place_kernel<<<blocks, kThreads, 0, stream>>>(N, pos, cell_of, rank, start, sorted);
-            rdf_cells_kernel<<<blocks, kThreads, shm, stream>>>(N, sorted, g, start, pp, rmax2, inv_dr, nbins, dh);
-            e = cudaGetLastError();
-            *launches += 6;
+Grid rdf_grid(const double L[3], double rmax, long long max_cells) {
+    // floor(L / rmax) in double: a tiny rmax gives a huge count, not an int overflow
+    double n[3];
+    for (int k = 0; k < 3; ++k) n[k] = std::max(1.0, std::floor(L[k] / rmax));
+    double prod = n[0] * n[1] * n[2];
+    if (prod > (double)max_cells) {
+        double f = std::cbrt((double)max_cells / prod);
+        for (int k = 0; k < 3; ++k) n[k] = std::max(1.0, std::floor(n[k] * f));
+        while (n[0] * n[1] * n[2] > (double)max_cells) {
+            int k = n[0] >= n[1] ? (n[0] >= n[2] ? 0 : 2) : (n[1] >= n[2] ? 1 : 2);
+            n[k] -= 1.0;
         }
     }
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(hist_host, dh, sizeof(unsigned long long) * nbins, cudaMemcpyDeviceToHost, stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-    cudaFree(dh);
-    cudaFree(cell_of);
-    cudaFree(rank);
-    cudaFree(count);
-    cudaFree(start);
-    cudaFree(tiles);
-    cudaFree(sorted);
-    if (e != cudaSuccess) {
-        std::snprintf(err, errlen, "rdf: %s", cudaGetErrorString(e));
-        return 2;  // LJ_ERR_CUDA
+    Grid g;
+    for (int k = 0; k < 3; ++k) {
+        g.n[k] = (int)n[k];
+        g.ratio[k] = (double)g.n[k] / L[k];
+    }
+    return g;
+}
+
+bool rdf_uses_cells(const Grid& g) { return g.n[0] >= 3 && g.n[1] >= 3 && g.n[2] >= 3; }
+
+int rdf_enqueue(int N, const double4* pos, const PairParams& pp, const Grid& g, int nbins, double rmax,
+                const RdfScratch& s, unsigned long long* hist, cudaStream_t stream, long long* launches) {
+    double rmax2 = rmax * rmax, inv_dr = (double)nbins / rmax;
+    size_t shm = sizeof(unsigned) * nbins;
+    int blocks = (N + kThreads - 1) / kThreads;
+    if (!rdf_uses_cells(g)) {
+        rdf_all_pairs_kernel<<<blocks, kThreads, shm, stream>>>(N, pos, pp, rmax2, inv_dr, nbins, hist);
+        ++*launches;
+        return cudaGetLastError() == cudaSuccess ? 0 : 2;
+    }
+    int nc = g.ncell();
+    int ntiles = (nc + kScanTile - 1) / kScanTile;
+    if (cudaMemsetAsync(s.count, 0, sizeof(int) * nc, stream) != cudaSuccess) return 2;
+    Gate open{};
+    open.always = 1;
+    rdf_bin_kernel<<<blocks, kThreads, 0, stream>>>(N, pos, g, s.cell_of, s.rank, s.count);
+    scan_reduce_kernel<false><<<ntiles, 1024, 0, stream>>>(s.count, nc, s.tiles, open);
+    scan_tiles_kernel<false><<<1, 1024, 0, stream>>>(s.tiles, ntiles, open);
+    scan_apply_kernel<false><<<ntiles, 1024, 0, stream>>>(s.count, nc, s.tiles, s.start, open);
+    rdf_place_kernel<<<blocks, kThreads, 0, stream>>>(N, pos, s.cell_of, s.rank, s.start, s.sorted);
+    rdf_cells_kernel<<<blocks, kThreads, shm, stream>>>(N, s.sorted, g, s.start, pp, rmax2, inv_dr, nbins, hist);
+    *launches += 6;
+    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+int rdf_set_smem(int nbins) {
+    size_t shm = sizeof(unsigned) * nbins;
+    if (shm <= 48 * 1024) return 0;
+    if (cudaFuncSetAttribute(rdf_cells_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm) != cudaSuccess ||
+        cudaFuncSetAttribute(rdf_all_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm) !=
+            cudaSuccess)
+        return 2;
+    return 0;
+}
+
+int rdf_reserve(RdfScratch& s, int N, int ncell, int nbins) {
+    if (N > s.atoms) {
+        cudaFree(s.cell_of);
+        cudaFree(s.rank);
+        cudaFree(s.sorted);
+        s.cell_of = s.rank = nullptr;
+        s.sorted = nullptr;
+        s.atoms = 0;
+        if (cudaMalloc(&s.cell_of, sizeof(int) * N) != cudaSuccess ||
+            cudaMalloc(&s.rank, sizeof(int) * N) != cudaSuccess ||
+            cudaMalloc(&s.sorted, sizeof(double4) * N) != cudaSuccess)
+            return 2;
+        s.atoms = N;
+    }
+    if (ncell > s.cells) {
+        cudaFree(s.count);
+        cudaFree(s.start);
+        s.count = s.start = nullptr;
+        s.cells = 0;
+        if (cudaMalloc(&s.count, sizeof(int) * ncell) != cudaSuccess ||
+            cudaMalloc(&s.start, sizeof(int) * (ncell + 1)) != cudaSuccess)
+            return 2;
+        s.cells = ncell;
+    }
+    if (!s.tiles && cudaMalloc(&s.tiles, sizeof(int) * kMaxScanTiles) != cudaSuccess) return 2;
+    if (nbins > s.bins) {
+        unsigned long long* h = nullptr;
+        if (cudaMalloc(&h, sizeof(unsigned long long) * 2 * (size_t)nbins) != cudaSuccess) return 2;
+        // a running accumulation moves to the new buffer (rare: a larger
+        // single sample taken in the middle of an accumulation)
+        // (the samples were enqueued on a non-blocking stream: wait for the device first)
+        if (s.samples > 0 &&
+            (cudaDeviceSynchronize() != cudaSuccess ||
+             cudaMemcpy(h, s.hist, sizeof(unsigned long long) * s.acc_bins, cudaMemcpyDeviceToDevice) != cudaSuccess)) {
+            cudaFree(h);
+            return 2;
+        }
+        cudaFree(s.hist);
+        s.hist = h;
+        s.bins = nbins;
     }
     return 0;
+}
+
+void rdf_release(RdfScratch& s) {
+    void* ptrs[] = {s.cell_of, s.rank, s.count, s.start, s.tiles, s.sorted, s.hist};
+    for (void* q : ptrs)
+        if (q) cudaFree(q);
+    s = RdfScratch{};
 }
 
 }  // namespace ljb
@@ -225,7 +263,12 @@ __device__ __align__(256) unsigned char g_rdf_scratch[kNoAllocBytes];
 constexpr int kMaxDevices = 64;
 std::atomic<unsigned char*> g_scratch_addr[kMaxDevices];
 
-// Device address of g_rdf_scratch on the current device (looked up once per device).
+// Device address of g_rdf_scratch on the current device, looked up on the
+// first call on each device and cached for the life of the process.  A
+// cudaDeviceReset (or anything else that destroys and recreates the device's
+// primary context) reloads the module and may move the array: the cached
+// address is then stale, so a process that resets a device must not call
+// lj_gpu_rdf_noalloc on it afterwards.
 int scratch_address(unsigned char** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 2;
@@ -249,52 +292,28 @@ extern "C" int lj_gpu_rdf_noalloc(const double* pos, int N, const double* box, i
     using namespace ljb;
     if (!pos || !box || !hist || N < 1 || nbins < 1 || !(rmax > 0)) return 1;  // LJ_ERR_ARG
     if (N > kNoAllocMaxAtoms || nbins > kNoAllocMaxBins) return 1;
-    if ((reinterpret_cast<uintptr_t>(pos) & 15) != 0) return 1;
+    // double4 position loads need 16-byte alignment, the 64-bit histogram atomics 8
+    if ((reinterpret_cast<uintptr_t>(pos) & 15) != 0 || (reinterpret_cast<uintptr_t>(hist) & 7) != 0) return 1;
     PairParams pp{};
     for (int k = 0; k < 3; ++k) {
-        if (!(box[k] > 0) || rmax > 0.5 * box[k]) return 1;
+        if (!(box[k] > 0) || !std::isfinite(box[k]) || rmax > 0.5 * box[k]) return 1;
         pp.L[k] = box[k];
         pp.halfL[k] = 0.5 * box[k];
     }
-    Grid g;
-    int nmin = 1 << 30;
-    for (int k = 0; k < 3; ++k) {
-        g.n[k] = (int)floor(pp.L[k] / rmax);
-        if (g.n[k] < 1) g.n[k] = 1;
-        g.ratio[k] = (double)g.n[k] / pp.L[k];
-        nmin = g.n[k] < nmin ? g.n[k] : nmin;
-    }
-    long long nc = (long long)g.n[0] * g.n[1] * g.n[2];
-    bool cells = nmin >= 3;
-    if (cells && nc > kNoAllocMaxCells) return 1;
+    // cells of edge >= rmax, coarser where the box holds more than the array's
+    // kNoAllocMaxCells of them (the histogram does not depend on the cell size)
+    Grid g = rdf_grid(pp.L, rmax, kNoAllocMaxCells);
     unsigned char* base = nullptr;
     if (scratch_address(&base)) return 2;  // LJ_ERR_CUDA
+    RdfScratch sc{};
+    sc.sorted = reinterpret_cast<double4*>(base + kOffSorted);
+    sc.cell_of = reinterpret_cast<int*>(base + kOffCellOf);
+    sc.rank = reinterpret_cast<int*>(base + kOffRank);
+    sc.count = reinterpret_cast<int*>(base + kOffCount);
+    sc.start = reinterpret_cast<int*>(base + kOffStart);
+    sc.tiles = reinterpret_cast<int*>(base + kOffTiles);
     cudaStream_t stream = static_cast<cudaStream_t>(stream_handle);
-    const double4* p4 = reinterpret_cast<const double4*>(pos);
-    double rmax2 = rmax * rmax, inv_dr = (double)nbins / rmax;
-    size_t shm = sizeof(unsigned) * nbins;
-    int blocks = (N + kThreads - 1) / kThreads;
     if (cudaMemsetAsync(hist, 0, sizeof(unsigned long long) * nbins, stream) != cudaSuccess) return 2;
-    if (!cells) {
-        rdf_all_pairs_kernel<<<blocks, kThreads, shm, stream>>>(N, p4, pp, rmax2, inv_dr, nbins, hist);
-    } else {
-        double4* sorted = reinterpret_cast<double4*>(base + kOffSorted);
-        int* cell_of = reinterpret_cast<int*>(base + kOffCellOf);
-        int* rank = reinterpret_cast<int*>(base + kOffRank);
-        int* count = reinterpret_cast<int*>(base + kOffCount);
-        int* start = reinterpret_cast<int*>(base + kOffStart);
-        int* tiles = reinterpret_cast<int*>(base + kOffTiles);
-        int ncell = (int)nc;
-        int ntiles = (ncell + kScanTile - 1) / kScanTile;
-        if (cudaMemsetAsync(count, 0, sizeof(int) * ncell, stream) != cudaSuccess) return 2;
-        Gate open{};
-        open.always = 1;
-        rdf_bin_kernel<<<blocks, kThreads, 0, stream>>>(N, p4, g, cell_of, rank, count);
-        scan_reduce_kernel<false><<<ntiles, 1024, 0, stream>>>(count, ncell, tiles, open);
-        scan_tiles_kernel<false><<<1, 1024, 0, stream>>>(tiles, ntiles, open);
-        scan_apply_kernel<false><<<ntiles, 1024, 0, stream>>>(count, ncell, tiles, start, open);
-        rdf_place_kernel<<<blocks, kThreads, 0, stream>>>(N, p4, cell_of, rank, start, sorted);
-        rdf_cells_kernel<<<blocks, kThreads, shm, stream>>>(N, sorted, g, start, pp, rmax2, inv_dr, nbins, hist);
-    }
-    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+    long long launches = 0;
+    return rdf_enqueue(N, reinterpret_cast<const double4*>(pos), pp, g, nbins, rmax, sc, hist, stream, &launches);
 }

@@ -128,6 +128,9 @@ SIGNATURES = {
     "lj_gpu_debug_cells": (ctypes.c_int, [P, P, P, P, P]),
     "lj_gpu_debug_pairs": (ctypes.c_longlong, [P, ctypes.c_longlong, P, P, P, P]),
     "lj_gpu_rdf": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double, P]),
+    "lj_gpu_rdf_accumulate": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double]),
+    "lj_gpu_rdf_read": (ctypes.c_int, [P, P, P]),
+    "lj_gpu_rdf_reset": (ctypes.c_int, [P]),
     "lj_gpu_get_stats": (ctypes.c_int, [P, P]),
     "lj_gpu_stream": (ctypes.c_void_p, [P]),
     "lj_gpu_step_async": (ctypes.c_int, [P, ctypes.c_int]),

@@ -218,9 +218,26 @@ class GpuSystem:
         return i, j, img, r2
 
     def rdf(self, nbins, rmax):
+        """Histogram of the current positions (ordered pairs, nbins bins on [0, rmax))."""
         h = np.zeros(nbins, dtype=np.uint64)
         self._check(nat.lib().lj_gpu_rdf(self._ctx, int(nbins), float(rmax), _p(h)))
         return h
+
+    def rdf_accumulate(self, nbins, rmax):
+        """Add the current positions' histogram to the device accumulator, without
+        waiting for it (no allocation after the first sample)."""
+        self._check(nat.lib().lj_gpu_rdf_accumulate(self._ctx, int(nbins), float(rmax)))
+        self._rdf_bins = int(nbins)
+
+    def rdf_read(self):
+        """(summed histogram, number of samples) of the accumulator."""
+        n = ctypes.c_longlong()
+        h = np.zeros(getattr(self, "_rdf_bins", 0), dtype=np.uint64)
+        self._check(nat.lib().lj_gpu_rdf_read(self._ctx, _p(h) if len(h) else None, ctypes.byref(n)))
+        return (h, n.value) if n.value else (np.zeros(0, dtype=np.uint64), 0)
+
+    def rdf_reset(self):
+        self._check(nat.lib().lj_gpu_rdf_reset(self._ctx))
 
     def stats(self):
         s = nat.Stats()

@@ -476,6 +476,24 @@ struct Window {
     }
 };
 
+// One ordered pair of the textbook RDF histogram: minimum-image separation
+// dd - image * L with image from dd > L/2, r^2 as sq_norm3, bin
+// floor(sqrt(r^2) * nbins / rmax).
+inline void rdf_count_pair(const double* pi, const double* pj, const double L[3], double rmax2, double inv_dr,
+                           int nbins, unsigned long long* hist) {
+    double s[3];
+    for (int k = 0; k < 3; ++k) {
+        double dd = pi[k] - pj[k];
+        double img = dd > 0.5 * L[k] ? 1.0 : (dd < -0.5 * L[k] ? -1.0 : 0.0);
+        s[k] = dd - img * L[k];
+    }
+    double r2 = sq_norm3(s);
+    if (r2 < rmax2) {
+        int b = static_cast<int>(std::sqrt(r2) * inv_dr);
+        if (b < nbins) hist[b]++;
+    }
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -658,20 +676,53 @@ int ljref_rdf(int N, const double* x, int stride, const double L[3], int nbins, 
     for (int i = 0; i < N; ++i)
         for (int j = 0; j < N; ++j) {
             if (i == j) continue;
-            const double* pi = x + (size_t)i * stride;
-            const double* pj = x + (size_t)j * stride;
-            double s[3];
-            for (int k = 0; k < 3; ++k) {
-                double dd = pi[k] - pj[k];
-                double img = dd > 0.5 * L[k] ? 1.0 : (dd < -0.5 * L[k] ? -1.0 : 0.0);
-                s[k] = dd - img * L[k];
-            }
-            double r2 = sq_norm3(s);
-            if (r2 < rmax2) {
-                int b = static_cast<int>(std::sqrt(r2) * inv_dr);
-                if (b < nbins) hist[b]++;
-            }
+            rdf_count_pair(x + (size_t)i * stride, x + (size_t)j * stride, L, rmax2, inv_dr, nbins, hist);
         }
+    return 0;
+}
+
+// The same histogram as ljref_rdf for large systems: the candidates of atom i
+// are the atoms of the 27 cells around its own on a grid of cells of edge
+// >= rmax (at least 3 per axis, so the 27 cells are distinct and hold every
+// atom within rmax); each ordered pair gets exactly ljref_rdf's arithmetic.
+// Atom ranges run on `threads` host threads with private histograms summed at
+// the end (integer counts: the sum is order-free).  Returns 1 if the box is
+// under 3 cells of edge rmax per axis.
+int ljref_rdf_cells(int N, const double* x, int stride, const double L[3], int nbins, double rmax,
+                    int threads, unsigned long long* hist) {
+    CellGrid g = make_grid(L, rmax);
+    if (g.n[0] < 3 || g.n[1] < 3 || g.n[2] < 3) return 1;
+    Cells c = bin_atoms(N, x, stride, g);
+    double rmax2 = rmax * rmax;
+    double inv_dr = static_cast<double>(nbins) / rmax;
+    if (threads < 1) threads = 1;
+    std::vector<std::vector<unsigned long long>> part(threads, std::vector<unsigned long long>(nbins, 0ULL));
+    auto work = [&](int t) {
+        unsigned long long* h = part[t].data();
+        for (int i = t; i < N; i += threads) {
+            int ci = c.cell_of[i];
+            int a = ci / (g.n[1] * g.n[2]), b = (ci / g.n[2]) % g.n[1], d = ci % g.n[2];
+            for (int da = -1; da <= 1; ++da)
+                for (int db = -1; db <= 1; ++db)
+                    for (int dd = -1; dd <= 1; ++dd) {
+                        int cell = g.flat((a + da + g.n[0]) % g.n[0], (b + db + g.n[1]) % g.n[1],
+                                          (d + dd + g.n[2]) % g.n[2]);
+                        for (int k = c.offsets[cell]; k < c.offsets[cell + 1]; ++k) {
+                            int j = c.members[k];
+                            if (j == i) continue;
+                            rdf_count_pair(x + (size_t)i * stride, x + (size_t)j * stride, L, rmax2, inv_dr,
+                                           nbins, h);
+                        }
+                    }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < threads; ++t) pool.emplace_back(work, t);
+    work(0);
+    for (auto& th : pool) th.join();
+    std::fill(hist, hist + nbins, 0ULL);
+    for (int t = 0; t < threads; ++t)
+        for (int b = 0; b < nbins; ++b) hist[b] += part[t][b];
     return 0;
 }
 

@@ -46,6 +46,7 @@ def lib(fast=False):
         L.ljref_run_steps.argtypes = [i, P, P, P, P, P, P, P, P, d, i, i, d, d, i, P]
         L.ljref_set_temperature.argtypes = [i, P, d]
         L.ljref_rdf.argtypes = [i, P, i, P, i, d, P]
+        L.ljref_rdf_cells.argtypes = [i, P, i, P, i, d, i, P]
         L.ljref_simulate.argtypes = [P, ll, P, P, i, P]
         L.ljref_simulate.restype = ll
         L.ljref_bench.argtypes = [i, d, d, u, d, d, i, i, i, P]
@@ -179,6 +180,18 @@ def rdf(x, L, nbins, rmax):
     x = as4(x)
     hist = np.zeros(nbins, dtype=np.uint64)
     lib().ljref_rdf(x.shape[0], _p(x), 4, _p(_box(L)), nbins, rmax, _p(hist))
+    return hist
+
+
+def rdf_cells(x, L, nbins, rmax, threads=None):
+    """ljref.rdf's histogram in O(N) through a cell list of edge >= rmax (boxes of
+    at least 3 such cells per axis), on `threads` host threads (default: all)."""
+    x = as4(x)
+    hist = np.zeros(nbins, dtype=np.uint64)
+    t = cpu_count() if threads is None else int(threads)
+    rc = lib().ljref_rdf_cells(x.shape[0], _p(x), 4, _p(_box(L)), nbins, rmax, t, _p(hist))
+    if rc != 0:
+        raise ValueError("rdf_cells needs at least 3 cells of edge rmax per axis")
     return hist
 
 

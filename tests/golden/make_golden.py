@@ -18,7 +18,9 @@ runs where that checkout exists) and writes:
   quick_single_run_run.ini     copy of run.ini
   quick_single_run_events.log  copy of events.log
 
-Usage:  python tests/golden/make_golden.py [reference_root]
+Usage:  python tests/golden/make_golden.py REFERENCE_ROOT
+
+REFERENCE_ROOT is the directory of a checkout of the reference repository.
 """
 
 import csv
@@ -37,7 +39,7 @@ def _rows(path, skip):
     return [[float(v) for v in r] for r in rows[skip:] if r]
 
 
-def main(ref_root="/root/reference"):
+def main(ref_root):
     data = pathlib.Path(ref_root) / "notebooks" / "quick_single_run" / "data"
     snap = np.array(_rows(data / "snapshots.csv", 2))  # two header rows
     assert snap.shape == (500, 11) and np.all(snap[:, 0] == 1600)
@@ -59,4 +61,6 @@ def main(ref_root="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    if len(sys.argv) != 2:
+        sys.exit(__doc__)
+    main(sys.argv[1])

@@ -121,12 +121,33 @@ def test_ctypes_structs_follow_the_header(name, cls):
         assert ftype == (base * int(m.group(2)) if m.group(2) else base)
 
 
-def test_integration_cython_params_follow_the_header():
-    """The Cython declaration shown for maintainers lists lj_params' fields in order."""
-    text = (ROOT / "INTEGRATION.md").read_text()
-    block = re.search(r"ctypedef struct lj_params:\n((?:        .*\n)+)", text).group(1)
-    shown = [" ".join(line.split()) for line in block.splitlines()]
-    assert shown == [f"{t} {f}" for t, f in _header_struct("lj_params")]
+def _pxd_struct(name):
+    """(type, field) lines of `ctypedef struct name:` in include/lj_gpu.pxd, in order."""
+    text = (ROOT / "include" / "lj_gpu.pxd").read_text()
+    block = re.search(r"ctypedef struct %s:\n((?:        .*\n)+)" % name, text).group(1)
+    return [" ".join(line.split()) for line in block.splitlines()]
+
+
+@pytest.mark.parametrize("name", ["lj_params", "lj_thermo"])
+def test_cython_declarations_follow_the_header(name):
+    """The Cython declarations a maintainer cimports list the header's fields in order and type."""
+    assert _pxd_struct(name) == [f"{t} {f}" for t, f in _header_struct(name)]
+
+
+def test_cython_functions_follow_the_header():
+    """Every function include/lj_gpu.pxd declares has the header's parameter and return types."""
+    text = (ROOT / "include" / "lj_gpu.pxd").read_text()
+    protos = _prototypes()
+    found = 0
+    for m in re.finditer(r"^    ([\w \*]+?)\b(lj_\w+)\(([^)]*)\)", text, flags=re.M):
+        ret, name, params = " ".join(m.group(1).split()), m.group(2), m.group(3)
+        want_ret, want_params = protos[name]
+        assert ret.replace(" *", "*") == want_ret.replace(" *", "*"), name
+        got = [" ".join(p.split()).replace(" *", "*") for p in params.split(",") if p.strip()]
+        want = [re.sub(r"\s*\b\w+$", "", p).replace(" *", "*") for p in want_params]
+        assert got == want, (name, got, want)
+        found += 1
+    assert found >= 10
 
 
 def _prototypes():

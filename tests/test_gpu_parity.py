@@ -285,6 +285,31 @@ def test_rdf_bit_exact(N, rho, rmax):
     assert np.array_equal(h, ljref.rdf(x, L, 200, rmax))
 
 
+def test_rdf_accumulates_on_the_device():
+    """Samples added on the device along a run equal the sum of single-sample
+    histograms of the same positions, each bit-exact with the oracle; a sample
+    with other bins is refused until a reset."""
+    from lennardjonesium._native import LJError
+    x, v, L = ljref.initial_state(4000, 1.2, 0.8, 7)
+    with gpu_system(4000, L) as g:
+        g.upload(x, v=v)
+        total = np.zeros(150, dtype=np.uint64)
+        for k in range(4):
+            g.step(25, record=False)
+            g.rdf_accumulate(150, 4.0)
+            h = g.rdf(150, 4.0)  # a single sample leaves the accumulation alone
+            assert np.array_equal(h, ljref.rdf(g.download()["x"], L, 150, 4.0))
+            total += h
+        acc, n = g.rdf_read()
+        assert n == 4 and np.array_equal(acc, total)
+        with pytest.raises(LJError):
+            g.rdf_accumulate(100, 4.0)
+        g.rdf_reset()
+        g.rdf_accumulate(100, 4.0)
+        acc, n = g.rdf_read()
+        assert n == 1 and np.array_equal(acc, g.rdf(100, 4.0))
+
+
 @pytest.mark.parametrize("per_pair", [False, True])
 def test_mixed_precision_force_error(per_pair):
     """Mixed path (FP32 pair arithmetic) vs FP64: stated bounds, with 8-pair FP32

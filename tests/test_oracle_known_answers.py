@@ -184,3 +184,14 @@ def test_rdf_ideal_lattice_peak():
     b1 = int(r1 * nbins / rmax)
     assert h[b1] == 256 * 12
     assert h[:b1].sum() == 0
+
+
+@pytest.mark.parametrize("N,rho,rmax,threads", [(2048, 0.8442, 3.0, 1), (4000, 0.8, 4.0, 3), (6912, 0.3, 5.0, 4)])
+def test_rdf_cells_equals_all_pairs(N, rho, rmax, threads):
+    """The O(N) cell-list RDF (used at sizes where the all-pairs one is too slow)
+    counts exactly the all-pairs histogram, on any number of threads."""
+    x, _, L = ljref.initial_state(N, 1.0, rho, 3)
+    rng = np.random.default_rng(N)
+    x[:, :3] = np.mod(x[:, :3] + rng.uniform(-0.3, 0.3, size=(N, 3)), L)
+    assert L / 3 >= rmax
+    assert np.array_equal(ljref.rdf_cells(x, L, 200, rmax, threads=threads), ljref.rdf(x, L, 200, rmax))
