@@ -97,6 +97,19 @@ typedef struct lj_thermo {
     double mean_square_displacement;
 } lj_thermo;
 
+/* One physics::ThermodynamicAnalyzer result (physics/analyzers.cpp:44-159):
+ * window means of T and TE, pressure rho (<T> + <W> / 3N), the
+ * microcanonical specific heat from the variance of T, and the diffusion
+ * coefficient from the MSD-vs-time slope. */
+typedef struct lj_observation {
+    double temperature;
+    double density;
+    double total_energy;
+    double pressure;
+    double specific_heat;
+    double diffusion_coefficient;
+} lj_observation;
+
 /* Counters describing the work done so far (for tests and tuning). */
 typedef struct lj_stats {
     long long steps;           /* velocity-Verlet steps taken */
@@ -191,6 +204,30 @@ int lj_gpu_rdf_read(lj_ctx* ctx, unsigned long long* hist, long long* samples);
 int lj_gpu_rdf_reset(lj_ctx* ctx);
 
 int lj_gpu_get_stats(const lj_ctx* ctx, lj_stats* out);
+
+/* ThermodynamicAnalyzer over the last sample_size step records, computed on
+ * the device from the context's record ring without copying the records:
+ * 2 <= sample_size <= 1024 (the ring) and <= the steps taken.  density is the
+ * system's rho (the analyzer's SystemParameters). */
+int lj_gpu_window_stats(lj_ctx* ctx, int sample_size, double density, lj_observation* out);
+
+/* The same analysis on the host over n records (oldest first), in the
+ * reference's summation order: the restatement the control protocol uses. */
+int lj_window_stats_host(const lj_thermo* records, int n, int particle_count, double density, lj_observation* out);
+
+/* Trajectory stream: the trajectory output the reference leaves as a TODO
+ * (control/simulation_controller.hpp:47-50), in the format of its snapshot
+ * file (output/sinks.cpp:162-204: two header rows, then one row
+ * "TimeStep,ParticleID,x,y,z,vx,vy,vz,fx,fy,fz" per atom in id order).
+ * After lj_gpu_trajectory_open, whenever lj_gpu_step or lj_gpu_step_async
+ * completes a step whose count (steps this context has taken) is a multiple
+ * of `every`, that state's frame is copied to pinned host memory on the
+ * context's stream and written by a background thread while the GPU runs on
+ * (two frames in flight at most).  lj_gpu_trajectory_close waits for every
+ * frame, closes the file and reports how many frames it holds (may be NULL).
+ * lj_gpu_destroy closes an open trajectory. */
+int lj_gpu_trajectory_open(lj_ctx* ctx, const char* path, int every);
+int lj_gpu_trajectory_close(lj_ctx* ctx, long long* frames);
 
 /* The context's CUDA stream (a cudaStream_t), for callers that time or order
  * work against it (e.g. torch.cuda.ExternalStream). */
@@ -360,6 +397,11 @@ int lj_batch_step(lj_batch* batch, int nsteps, lj_thermo* out);
 int lj_batch_measure(lj_batch* batch, lj_thermo* out);
 /* physics::set_temperature for one system (transformations.cpp:94-116). */
 int lj_batch_set_temperature(lj_batch* batch, int sys, double target, double* measured);
+/* ThermodynamicAnalyzer of every system over the last sample_size batch steps
+ * (2 <= sample_size <= 256, the batch's record ring), on the device, one block
+ * per system: density[nsys] in, out[nsys] receives each system's result.  A
+ * system inactive during part of the window keeps its older records there. */
+int lj_batch_window_stats(lj_batch* batch, int sample_size, const double* density, lj_observation* out);
 /* Totals for tests and tuning: atoms, neighbour-list builds per system, direct kernel launches. */
 int lj_batch_info(const lj_batch* batch, int* total_atoms, long long* builds_per_system, long long* kernel_launches);
 

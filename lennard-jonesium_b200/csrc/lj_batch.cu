@@ -446,6 +446,8 @@ struct lj_batch {
     int *ids = nullptr, *ids_tmp = nullptr, *cell_of = nullptr, *rank = nullptr, *order = nullptr;
     int *count = nullptr, *start = nullptr, *cnt = nullptr;
     uint4* nbr = nullptr;
+    double* dstats = nullptr;  // window statistics: nsys x 6 results, then nsys densities
+    int* natoms = nullptr;     // atoms per system
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
     bool graph_tried = false;
@@ -626,7 +628,7 @@ int read_flags_b(lj_batch* b) {
 void free_b(lj_batch* b) {
     void* ptrs[] = {b->sys, b->st, b->fl, b->blk_sys, b->blk_first, b->sys_of, b->cell_sys, b->pos, b->pos_tmp,
                     b->posf, b->soa, b->soa_tmp, b->bd, b->partials, b->ring, b->ids, b->ids_tmp, b->cell_of,
-                    b->rank, b->order, b->count, b->start, b->cnt, b->nbr};
+                    b->rank, b->order, b->count, b->start, b->cnt, b->nbr, b->dstats, b->natoms};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (b->host_ring) cudaFreeHost(b->host_ring);
@@ -743,6 +745,13 @@ int lj_batch_create(const lj_batch_system* systems, int nsys, double cutoff, int
         BK(cudaMalloc(&b->start, sizeof(int) * (ncell + 1)));
         BK(cudaMalloc(&b->cnt, sizeof(int) * N));
         BK(cudaMalloc(&b->nbr, sizeof(uint4) * (size_t)(b->cap / 4) * N));
+        BK(cudaMalloc(&b->dstats, sizeof(double) * 7 * nsys));
+        BK(cudaMalloc(&b->natoms, sizeof(int) * nsys));
+        {
+            std::vector<int> na((size_t)nsys);
+            for (int s = 0; s < nsys; ++s) na[(size_t)s] = b->hsys[(size_t)s].natoms;
+            BK(cudaMemcpy(b->natoms, na.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice));
+        }
         BK(cudaMemcpy(b->sys, b->hsys.data(), sizeof(SysDev) * nsys, cudaMemcpyHostToDevice));
         std::vector<SysState> st0((size_t)nsys);
         for (auto& q : st0) {
@@ -913,6 +922,21 @@ int lj_batch_set_temperature(lj_batch* b, int sys, double target, double* measur
     Soa s{b->soa, b->Ntot};
     b_scale_kernel<<<nb(S.natoms), kThreads, 0, b->stream>>>(S.atom_off, S.natoms, s, std::sqrt(target / T));
     BKL();
+    BK(cudaStreamSynchronize(b->stream));
+    return LJ_OK;
+}
+
+int lj_batch_window_stats(lj_batch* b, int sample_size, const double* density, lj_observation* out) {
+    if (!b || !density || !out || sample_size < 2 || sample_size > b->ring_cap || sample_size > b->host_steps)
+        return LJ_ERR_ARG;
+    BK(cudaSetDevice(b->device));
+    double* dens = b->dstats + 6 * (size_t)b->nsys;
+    BK(cudaMemcpyAsync(dens, density, sizeof(double) * b->nsys, cudaMemcpyHostToDevice, b->stream));
+    window_stats_kernel<<<b->nsys, kStatsThreads, 0, b->stream>>>(b->ring, b->ring_cap, b->nsys, b->host_steps - 1,
+                                                                 sample_size, b->natoms, dens, b->dstats);
+    BKL();
+    static_assert(sizeof(lj_observation) == 6 * sizeof(double), "lj_observation is 6 doubles");
+    BK(cudaMemcpyAsync(out, b->dstats, sizeof(double) * 6 * b->nsys, cudaMemcpyDeviceToHost, b->stream));
     BK(cudaStreamSynchronize(b->stream));
     return LJ_OK;
 }

@@ -11,10 +11,14 @@
 
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <deque>
+#include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -25,6 +29,8 @@
 #include "lj_tile.cuh"
 
 using namespace ljb;
+
+struct Trajectory;  // the trajectory stream (below)
 
 // One instantiated step graph.
 struct StepGraph {
@@ -71,6 +77,7 @@ struct lj_ctx {
     double* ring = nullptr;     // ring_cap records of 7 doubles
     double* dscratch = nullptr; // small device scratch (set_temperature factor, L)
     double* dL = nullptr;
+    double* dstats = nullptr;   // window statistics: 6 results, density, atom count
     int ring_cap = 0;
     double* host_ring = nullptr;  // pinned
 
@@ -97,6 +104,7 @@ struct lj_ctx {
     int* dbg_tiles = nullptr;
     // RDF cell-list scratch and device accumulator, sized on first use
     RdfScratch rdf{};
+    Trajectory* traj = nullptr;  // open trajectory stream, if any
 
     long long launches = 0;       // kernels launched directly (gated-off ones included)
     long long host_steps = 0;     // mirror of the device step counter
@@ -525,7 +533,7 @@ int build_step_graph(lj_ctx* ctx, int nsteps, StepGraph& out) {
 constexpr int kGraphSteps[2] = {32, 8};
 
 // Enqueue nsteps steps: whole step graphs where available, single launches for the rest.
-int enqueue_steps(lj_ctx* ctx, int nsteps) {
+int enqueue_run(lj_ctx* ctx, int nsteps) {
     if (!ctx->graph_tried) {
         ctx->graph_tried = true;
         for (int q = 0; q < 2; ++q)
@@ -547,6 +555,148 @@ int enqueue_steps(lj_ctx* ctx, int nsteps) {
     return LJ_OK;
 }
 
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Trajectory stream: every `every` steps the state (x, v, F in atom-id order)
+// is packed on the device, copied with one cudaMemcpyAsync into one of two
+// pinned host buffers, and a writer thread formats it in the snapshot format
+// of output/sinks.cpp:162-204 while the GPU runs on.  The enqueueing thread
+// waits only when both buffers are still being written out.
+// ---------------------------------------------------------------------------
+static __global__ void __launch_bounds__(kThreads)
+frame_pack_kernel(int N, const double4* __restrict__ pos, Soa s, const int* __restrict__ ids,
+                  double* __restrict__ out) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= N) return;
+    double* o = out + 9 * (size_t)ids[k];
+    double4 x = pos[k];
+    o[0] = x.x;
+    o[1] = x.y;
+    o[2] = x.z;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        o[3 + q] = s.at(VX + q, k);
+        o[6 + q] = s.at(FX + q, k);
+    }
+}
+
+namespace ljb {
+// Snapshot rows of n atoms (x, y, z, vx, vy, vz, fx, fy, fz each) at time_step (lj_sim.cpp).
+int write_snapshot_rows(long long time_step, const double* xvf, int n, FILE* f);
+}  // namespace ljb
+
+struct Trajectory {
+    FILE* f = nullptr;
+    int every = 1;
+    int N = 0;
+    int device = 0;
+    double* dstage = nullptr;      // N x 9 doubles on the device
+    double* host[2] = {nullptr, nullptr};  // pinned frames
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    long long step_of[2] = {0, 0};
+    bool busy[2] = {false, false};  // queued for, or being written by, the writer
+    int next = 0;
+    long long frames = 0;
+    int error = 0;  // a write failed
+    std::mutex m;
+    std::condition_variable cv;
+    std::deque<int> q;
+    bool stop = false;
+    std::thread th;
+
+    void run() {
+        cudaSetDevice(device);
+        for (;;) {
+            int b;
+            {
+                std::unique_lock<std::mutex> g(m);
+                cv.wait(g, [this] { return stop || !q.empty(); });
+                if (q.empty()) return;
+                b = q.front();
+                q.pop_front();
+            }
+            int err = cudaEventSynchronize(ev[b]) != cudaSuccess ||
+                      write_snapshot_rows(step_of[b], host[b], N, f) != 0;
+            {
+                std::lock_guard<std::mutex> g(m);
+                busy[b] = false;
+                if (err) error = 1;
+            }
+            cv.notify_all();
+        }
+    }
+    // wait until every queued frame is written
+    void drain() {
+        std::unique_lock<std::mutex> g(m);
+        cv.wait(g, [this] { return q.empty() && !busy[0] && !busy[1]; });
+    }
+};
+
+namespace {
+
+void traj_close(Trajectory* t) {
+    if (!t) return;
+    if (t->th.joinable()) {
+        t->drain();
+        {
+            std::lock_guard<std::mutex> g(t->m);
+            t->stop = true;
+        }
+        t->cv.notify_all();
+        t->th.join();
+    }
+    if (t->f) std::fclose(t->f);
+    for (int b = 0; b < 2; ++b) {
+        if (t->host[b]) cudaFreeHost(t->host[b]);
+        if (t->ev[b]) cudaEventDestroy(t->ev[b]);
+    }
+    if (t->dstage) cudaFree(t->dstage);
+    delete t;
+}
+
+// Enqueue the frame of the current state (step count ctx->host_steps).
+int traj_frame(lj_ctx* ctx) {
+    Trajectory* t = ctx->traj;
+    int b = t->next;
+    {
+        std::unique_lock<std::mutex> g(t->m);
+        t->cv.wait(g, [&] { return !t->busy[b]; });
+    }
+    frame_pack_kernel<<<ctx->nblocks, kThreads, 0, ctx->stream>>>(ctx->N, ctx->pos, soa_of(ctx->soa, ctx->N),
+                                                                   ctx->ids, t->dstage);
+    CKL();
+    CK(cudaMemcpyAsync(t->host[b], t->dstage, sizeof(double) * 9 * (size_t)ctx->N, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaEventRecord(t->ev[b], ctx->stream));
+    {
+        std::lock_guard<std::mutex> g(t->m);
+        t->busy[b] = true;
+        t->step_of[b] = ctx->host_steps;
+        t->q.push_back(b);
+    }
+    t->cv.notify_all();
+    t->next = b ^ 1;
+    ++t->frames;
+    return LJ_OK;
+}
+
+// Enqueue nsteps steps, stopping at every step count that is a multiple of the
+// trajectory interval to enqueue its frame.
+int enqueue_steps(lj_ctx* ctx, int nsteps) {
+    if (!ctx->traj) return enqueue_run(ctx, nsteps);
+    int done = 0;
+    while (done < nsteps) {
+        long long every = ctx->traj->every;
+        int n = (int)std::min<long long>(nsteps - done, every - ctx->host_steps % every);
+        int rc = enqueue_run(ctx, n);
+        if (rc) return rc;
+        done += n;
+        if (ctx->host_steps % every == 0 && (rc = traj_frame(ctx))) return rc;
+    }
+    return LJ_OK;
+}
+
 int read_flags(lj_ctx* ctx) {
     Scalars h;
     CK(cudaMemcpyAsync(&h, ctx->sc, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
@@ -559,12 +709,14 @@ int read_flags(lj_ctx* ctx) {
 void free_all(lj_ctx* c) {
     void* ptrs[] = {c->posf, c->pos, c->pos_tmp, c->soa, c->soa_tmp, c->bd, c->ids, c->ids_tmp, c->cell_of,
                     c->rank, c->order, c->count, c->start, c->tile_sums, c->nbr, c->cnt, c->partials,
-                    c->sc, c->ring, c->dscratch, c->posl, c->bx, c->nbr8, c->pos_b, c->posl_b, c->dbg_count,
+                    c->sc, c->ring, c->dscratch, c->dstats, c->posl, c->bx, c->nbr8, c->pos_b, c->posl_b, c->dbg_count,
                     c->dbg_start,
                     c->dbg_members, c->dbg_cell_of, c->dbg_tiles};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     rdf_release(c->rdf);
+    traj_close(c->traj);
+    c->traj = nullptr;
     if (c->host_ring) cudaFreeHost(c->host_ring);
     for (StepGraph& g : c->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -683,6 +835,7 @@ int init_ctx(lj_ctx* ctx, const lj_params& p) {
     ctx->ring_cap = 1024;
     CK(cudaMalloc(&ctx->ring, sizeof(double) * 7 * (ctx->ring_cap + 1)));
     CK(cudaMalloc(&ctx->dscratch, sizeof(double) * 8));
+    CK(cudaMalloc(&ctx->dstats, sizeof(double) * 8));
     ctx->dL = ctx->dscratch + 4;
     CK(cudaMallocHost(&ctx->host_ring, sizeof(double) * 7 * ctx->ring_cap));
     if (p.precision == LJ_PRECISION_MIXED) {
@@ -1202,6 +1355,73 @@ int lj_gpu_step_timed(lj_ctx* ctx, int nsteps, lj_phase_times* out) {
 }  // extern "C"
 
 extern "C" {
+
+int lj_gpu_window_stats(lj_ctx* ctx, int sample_size, double density, lj_observation* out) {
+    if (!ctx || !out || sample_size < 2 || sample_size > ctx->ring_cap || sample_size > ctx->host_steps)
+        return set_err(ctx, LJ_ERR_ARG, "window_stats: need 2 <= sample_size <= min(1024, steps taken)");
+    CK(cudaSetDevice(ctx->p.device));
+    double in[2];
+    int n = ctx->N;
+    in[0] = density;
+    std::memcpy(&in[1], &n, sizeof n);
+    CK(cudaMemcpyAsync(ctx->dstats + 6, in, sizeof in, cudaMemcpyHostToDevice, ctx->stream));
+    window_stats_kernel<<<1, kStatsThreads, 0, ctx->stream>>>(ctx->ring, ctx->ring_cap, 1, ctx->host_steps - 1,
+                                                             sample_size, reinterpret_cast<int*>(ctx->dstats + 7),
+                                                             ctx->dstats + 6, ctx->dstats);
+    CKL();
+    double o[6];
+    CK(cudaMemcpyAsync(o, ctx->dstats, sizeof o, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    *out = lj_observation{o[0], o[1], o[2], o[3], o[4], o[5]};
+    return LJ_OK;
+}
+
+int lj_gpu_trajectory_open(lj_ctx* ctx, const char* path, int every) {
+    if (!ctx || !path || every < 1) return set_err(ctx, LJ_ERR_ARG, "bad trajectory arguments");
+    if (ctx->traj) return set_err(ctx, LJ_ERR_ARG, "a trajectory is already open");
+    CK(cudaSetDevice(ctx->p.device));
+    Trajectory* t = new (std::nothrow) Trajectory();
+    if (!t) return set_err(ctx, LJ_ERR_ARG, "out of host memory");
+    t->every = every;
+    t->N = ctx->N;
+    t->device = ctx->p.device;
+    size_t bytes = sizeof(double) * 9 * (size_t)ctx->N;
+    t->f = std::fopen(path, "w");
+    int rc = LJ_OK;
+    if (!t->f) {
+        rc = set_err(ctx, LJ_ERR_ARG, "cannot open the trajectory file");
+    } else if (cudaMalloc(&t->dstage, bytes) != cudaSuccess || cudaMallocHost(&t->host[0], bytes) != cudaSuccess ||
+               cudaMallocHost(&t->host[1], bytes) != cudaSuccess ||
+               cudaEventCreateWithFlags(&t->ev[0], cudaEventDisableTiming) != cudaSuccess ||
+               cudaEventCreateWithFlags(&t->ev[1], cudaEventDisableTiming) != cudaSuccess) {
+        rc = set_err(ctx, LJ_ERR_CUDA, "trajectory buffers: allocation failed");
+    } else {
+        // the two header rows of output/sinks.cpp:162-183
+        std::fputs("TimeStep,ParticleID,Position,Position,Position,Velocity,Velocity,Velocity,Force,Force,Force\n"
+                   "TimeStep,ParticleID,X,Y,Z,X,Y,Z,X,Y,Z\n",
+                   t->f);
+        t->th = std::thread([t] { t->run(); });
+    }
+    if (rc) {
+        traj_close(t);
+        return rc;
+    }
+    ctx->traj = t;
+    return LJ_OK;
+}
+
+int lj_gpu_trajectory_close(lj_ctx* ctx, long long* frames) {
+    if (!ctx) return LJ_ERR_ARG;
+    Trajectory* t = ctx->traj;
+    if (!t) return set_err(ctx, LJ_ERR_ARG, "no trajectory is open");
+    CK(cudaSetDevice(ctx->p.device));
+    t->drain();
+    int err = t->error;
+    if (frames) *frames = t->frames;
+    ctx->traj = nullptr;
+    traj_close(t);
+    return err ? set_err(ctx, LJ_ERR_ARG, "trajectory: a frame could not be written") : LJ_OK;
+}
 
 // Project autotuner: for the caller's system (base params + state), time
 // `steps` velocity-Verlet steps for every candidate and return the fastest

@@ -796,6 +796,63 @@ finalize_kernel(const double* __restrict__ partials, int nblocks, int N, double 
     }
 }
 
+// ThermodynamicAnalyzer::result (analyzers.cpp:44-159) over the last W step
+// records of a record ring, one block per system: record k of the window
+// (k = 0 oldest) of system s sits at ring + 7 * (slot(k) * nsys + s) with
+// slot(k) = (last - (W - 1) + k) mod ring_cap.  Two passes as
+// tools::MovingSample::statistics (moving_sample.hpp:107-188): the means, then
+// the Bessel-corrected variance of T and the covariance of (t, MSD); each sum
+// is a fixed-order block reduction.
+constexpr int kStatsThreads = 256;
+
+static __global__ void __launch_bounds__(kStatsThreads)
+window_stats_kernel(const double* __restrict__ ring, int ring_cap, int nsys, long long last, int W,
+                    const int* __restrict__ natoms, const double* __restrict__ density, double* __restrict__ out) {
+    int s = blockIdx.x;
+    auto rec = [&](int k) {
+        long long step = last - (W - 1) + k;
+        int slot = (int)(((step % ring_cap) + ring_cap) % ring_cap);
+        return ring + 7 * ((size_t)slot * nsys + s);
+    };
+    // pass 1: sums of T, TE, W, t, MSD
+    double a[5] = {0, 0, 0, 0, 0};
+    for (int k = threadIdx.x; k < W; k += kStatsThreads) {
+        const double* r = rec(k);
+        a[0] += r[5];
+        a[1] += r[3];
+        a[2] += r[4];
+        a[3] += r[0];
+        a[4] += r[6];
+    }
+    block_sum<5, kStatsThreads>(a);
+    __shared__ double mean[5];
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 5; ++q) mean[q] = a[q] / (double)W;
+    __syncthreads();
+    // pass 2: sum (T - <T>)^2, (t - <t>)(MSD - <MSD>), (t - <t>)^2
+    double c[3] = {0, 0, 0};
+    for (int k = threadIdx.x; k < W; k += kStatsThreads) {
+        const double* r = rec(k);
+        double dT = r[5] - mean[0], dt = r[0] - mean[3], dm = r[6] - mean[4];
+        c[0] += dT * dT;
+        c[1] += dt * dm;
+        c[2] += dt * dt;
+    }
+    block_sum<3, kStatsThreads>(c);
+    if (threadIdx.x == 0) {
+        double N = (double)natoms[s], rho = density[s];
+        double T = mean[0];
+        double varT = c[0] / (double)(W - 1);
+        double* o = out + 6 * (size_t)s;
+        o[0] = T;
+        o[1] = rho;
+        o[2] = mean[1];
+        o[3] = rho * (T + mean[2] / (3.0 * N));
+        o[4] = (3. / 2.) / (1 - (3. / 2.) * N * (varT / (T * T)));
+        o[5] = (1. / 6.) * ((c[1] / (double)(W - 1)) / (c[2] / (double)(W - 1)));
+    }
+}
+
 // Graph step: decide on the device whether the rebuild subgraph runs this step.
 static __global__ void decide_rebuild_kernel(Gate gate, cudaGraphConditionalHandle h, Scalars* sc) {
     bool open = gate.open();

@@ -287,7 +287,54 @@ double relative_error(double measured, double desired) { return std::abs(measure
 
 }  // namespace
 
+namespace ljb {
+
+// Rows of the snapshot file (output/sinks.cpp:185-204): "step,id,x,y,z,vx,vy,vz,fx,fy,fz"
+// for atoms 0..n-1 of xvf (9 doubles per atom).  Returns 0, or 1 if a write failed.
+int write_snapshot_rows(long long time_step, const double* xvf, int n, FILE* f) {
+    std::vector<char> buf;
+    buf.reserve(1 << 20);
+    char line[400];
+    for (int i = 0; i < n; ++i) {
+        char* o = line;
+        o = std::to_chars(o, o + 24, time_step).ptr;
+        *o++ = ',';
+        o = std::to_chars(o, o + 16, i).ptr;
+        for (int k = 0; k < 9; ++k) {
+            *o++ = ',';
+            o += fmt_double_buf(xvf[9 * (size_t)i + k], o);
+        }
+        *o++ = '\n';
+        buf.insert(buf.end(), line, o);
+        if (buf.size() > (1 << 20) - 512) {
+            if (std::fwrite(buf.data(), 1, buf.size(), f) != buf.size()) return 1;
+            buf.clear();
+        }
+    }
+    if (!buf.empty() && std::fwrite(buf.data(), 1, buf.size(), f) != buf.size()) return 1;
+    return std::fflush(f) == 0 ? 0 : 1;
+}
+
+}  // namespace ljb
+
 extern "C" {
+
+int lj_window_stats_host(const lj_thermo* records, int n, int particle_count, double density, lj_observation* out) {
+    if (!records || !out || n < 2 || particle_count < 1) return LJ_ERR_ARG;
+    Window T(n), E(n), W(n), t(n), msd(n);
+    for (int k = 0; k < n; ++k) {
+        const lj_thermo& r = records[k];
+        T.push(r.temperature);
+        E.push(r.total_energy);
+        W.push(r.virial);
+        t.push(r.time);
+        msd.push(r.mean_square_displacement);
+    }
+    Observation o = analyze(T, E, W, t, msd, particle_count, density);
+    *out = lj_observation{o.temperature, o.density, o.total_energy, o.pressure, o.specific_heat,
+                          o.diffusion_coefficient};
+    return LJ_OK;
+}
 
 int lj_format_double(double v, char* out, int cap) {
     if (!out || cap < 1) return LJ_ERR_ARG;

@@ -99,6 +99,11 @@ class AdjParams(ctypes.Structure):
                 ("device", ctypes.c_int)]
 
 
+class Observation(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in (
+        "temperature", "density", "total_energy", "pressure", "specific_heat", "diffusion_coefficient")]
+
+
 class LJError(RuntimeError):
     """A C-ABI call returned a non-zero status."""
 
@@ -132,6 +137,11 @@ SIGNATURES = {
     "lj_gpu_rdf_read": (ctypes.c_int, [P, P, P]),
     "lj_gpu_rdf_reset": (ctypes.c_int, [P]),
     "lj_gpu_get_stats": (ctypes.c_int, [P, P]),
+    "lj_gpu_window_stats": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double, P]),
+    "lj_window_stats_host": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, ctypes.c_double, P]),
+    "lj_batch_window_stats": (ctypes.c_int, [P, ctypes.c_int, P, P]),
+    "lj_gpu_trajectory_open": (ctypes.c_int, [P, ctypes.c_char_p, ctypes.c_int]),
+    "lj_gpu_trajectory_close": (ctypes.c_int, [P, P]),
     "lj_gpu_stream": (ctypes.c_void_p, [P]),
     "lj_gpu_step_async": (ctypes.c_int, [P, ctypes.c_int]),
     "lj_gpu_synchronize": (ctypes.c_int, [P]),

@@ -239,6 +239,16 @@ class GpuSystem:
     def rdf_reset(self):
         self._check(nat.lib().lj_gpu_rdf_reset(self._ctx))
 
+    def trajectory_open(self, path, every):
+        """Write a frame (snapshot format) every `every` steps to `path` while stepping."""
+        self._check(nat.lib().lj_gpu_trajectory_open(self._ctx, str(path).encode(), int(every)))
+
+    def trajectory_close(self):
+        """Flush and close the trajectory; returns the number of frames written."""
+        n = ctypes.c_longlong()
+        self._check(nat.lib().lj_gpu_trajectory_close(self._ctx, ctypes.byref(n)))
+        return n.value
+
     def stats(self):
         s = nat.Stats()
         self._check(nat.lib().lj_gpu_get_stats(self._ctx, ctypes.byref(s)))

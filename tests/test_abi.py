@@ -190,3 +190,25 @@ def test_signatures_follow_the_header():
         for a, prm in zip(args, params):
             k = _kind(prm)
             assert as_kind[a] == k or (k == "char_p" and as_kind[a] == "ptr"), (name, prm)
+
+
+def test_window_stats_host_matches_the_analyzer_formulas():
+    """lj_window_stats_host restates physics/analyzers.cpp:44-159 over records
+    (no GPU): numpy's two-pass statistics agree to 1e-12."""
+    from lennardjonesium import _native
+    rng = np.random.default_rng(7)
+    n, N, rho = 300, 4000, 0.8
+    rec = np.zeros((n, 7))
+    rec[:, 0] = 0.005 * np.arange(1, n + 1)
+    rec[:, 5] = 1.2 + 0.01 * rng.standard_normal(n)
+    rec[:, 3] = -4000 + rng.standard_normal(n)
+    rec[:, 4] = 2000 + 10 * rng.standard_normal(n)
+    rec[:, 6] = 0.3 * rec[:, 0] + 1e-3 * rng.standard_normal(n)
+    o = _native.Observation()
+    assert _native.lib().lj_window_stats_host(rec.ctypes.data_as(ctypes.c_void_p), n, N, rho, ctypes.byref(o)) == 0
+    T = rec[:, 5].mean()
+    varT = rec[:, 5].var(ddof=1)
+    want = [T, rho, rec[:, 3].mean(), rho * (T + rec[:, 4].mean() / (3 * N)),
+            1.5 / (1 - 1.5 * N * varT / T ** 2), np.cov(rec[:, 0], rec[:, 6])[0, 1] / rec[:, 0].var(ddof=1) / 6]
+    got = [getattr(o, f) for f, _ in o._fields_]
+    assert np.allclose(got, want, rtol=1e-12, atol=0)

@@ -108,3 +108,38 @@ def test_run_sweep_small_grid(tmp_path):
         assert lj.Configuration.from_file(folder / "run.ini").system.random_seed == 11
         for name in ("events.log", "thermodynamics.csv", "observations.csv", "snapshots.csv"):
             assert (folder / name).is_file()
+
+
+def _fmt(v):
+    import ctypes
+    from lennardjonesium import _native as nat
+    buf = ctypes.create_string_buffer(40)
+    assert nat.lib().lj_format_double(float(v), buf, 40) == 0
+    return buf.value.decode()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_trajectory_frames_equal_downloads(tmp_path, precision):
+    """Each trajectory frame, written by the background writer while the GPU
+    steps on, is byte for byte the snapshot rows of lj_gpu_download_state at
+    that step (steps 10, 20, 30 with every = 10; the 7 steps after the last
+    frame add none)."""
+    from lennardjonesium import GpuSystem
+    N = 500
+    x, v, L = ljref.initial_state(N, 0.5, 0.8, 117208264)
+    path = tmp_path / "trajectory.csv"
+    want = ["TimeStep,ParticleID,Position,Position,Position,Velocity,Velocity,Velocity,Force,Force,Force",
+            "TimeStep,ParticleID,X,Y,Z,X,Y,Z,X,Y,Z"]
+    with GpuSystem(N, L, precision=precision) as g:
+        g.upload(x, v=v)
+        g.trajectory_open(path, 10)
+        for step in (10, 20, 30):
+            g.step(10, record=False)
+            st = g.download()
+            for i in range(N):
+                vals = [st[k][i, q] for k in ("x", "v", "F") for q in range(3)]
+                want.append(",".join([str(step), str(i)] + [_fmt(a) for a in vals]))
+        g.step_async(7)
+        g.synchronize()
+        assert g.trajectory_close() == 3
+    assert path.read_text() == "\n".join(want) + "\n"

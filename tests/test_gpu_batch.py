@@ -122,3 +122,60 @@ def test_run_sweep_batched_equals_thread_pool(tmp_path):
             a, p = tmp_path / "batched" / sub / name, tmp_path / "pool" / sub / name
             assert filecmp.cmp(a, p, shallow=False), f"{sub}/{name}"
     assert len(runs["batched"].completed) == len(runs["pool"].completed)
+
+
+def _host_stats(records, N, rho):
+    from lennardjonesium import _native as nat
+    r = np.ascontiguousarray(records, dtype=np.float64)
+    o = nat.Observation()
+    assert nat.lib().lj_window_stats_host(r.ctypes.data_as(ctypes.c_void_p), r.shape[0], N, rho,
+                                          ctypes.byref(o)) == 0
+    return np.array([getattr(o, f) for f, _ in o._fields_])
+
+
+def test_batch_window_statistics_on_device():
+    """ThermodynamicAnalyzer results of 64 systems computed on the device from the
+    batch's record ring equal the host restatement over the same records to 1e-12."""
+    from lennardjonesium import _native as nat
+    rng = np.random.default_rng(64)
+    states, L, sizes, rhos = [], [], [], []
+    for k in range(64):
+        n = int(rng.integers(5, 9))
+        rho = float(rng.uniform(0.3, 1.0))
+        x, v, box = ljref.initial_state(4 * n ** 3, float(rng.uniform(0.5, 2.0)), rho, 100 + k)
+        states.append((x, v))
+        L.append(box)
+        sizes.append(4 * n ** 3)
+        rhos.append(rho)
+    lib, b = _batch(states, L)
+    try:
+        W = 200
+        recs = np.zeros((250, 64, 7))
+        assert lib.lj_batch_step(b, 250, recs.ctypes.data_as(ctypes.c_void_p)) == 0
+        obs = (nat.Observation * 64)()
+        dens = np.array(rhos)
+        assert lib.lj_batch_window_stats(b, W, dens.ctypes.data_as(ctypes.c_void_p), obs) == 0
+        assert lib.lj_batch_window_stats(b, 300, dens.ctypes.data_as(ctypes.c_void_p), obs) == nat.LJ_ERR_ARG
+        assert lib.lj_batch_window_stats(b, W, dens.ctypes.data_as(ctypes.c_void_p), obs) == 0
+    finally:
+        lib.lj_batch_destroy(b)
+    for s in range(64):
+        want = _host_stats(recs[-W:, s, :], sizes[s], rhos[s])
+        got = np.array([getattr(obs[s], f) for f, _ in obs[s]._fields_])
+        assert np.all(np.abs(got - want) <= 1e-12 * np.abs(want)), (s, got, want)
+
+
+def test_context_window_statistics_on_device():
+    from lennardjonesium import GpuSystem
+    from lennardjonesium import _native as nat
+    x, v, L = ljref.initial_state(4000, 1.2, 0.8, 7)
+    with GpuSystem(4000, L) as g:
+        g.upload(x, v=v)
+        recs = g.step(1300)  # the ring holds the last 1024 records
+        o = nat.Observation()
+        for W in (2, 500, 1024):
+            assert nat.lib().lj_gpu_window_stats(g._ctx, W, 0.8, ctypes.byref(o)) == 0
+            got = np.array([getattr(o, f) for f, _ in o._fields_])
+            want = _host_stats(recs[-W:], 4000, 0.8)
+            assert np.all(np.abs(got - want) <= 1e-12 * np.abs(want)), (W, got, want)
+        assert nat.lib().lj_gpu_window_stats(g._ctx, 1025, 0.8, ctypes.byref(o)) == nat.LJ_ERR_ARG
