@@ -449,7 +449,6 @@ def run_sweep_bench(args):
     lib = nat.lib()
     P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
 
-    # batched
     table = (nat.BatchSystem * nsys)()
     for s, sy in enumerate(systems):
         table[s].particle_count = sy["N"]
@@ -457,8 +456,19 @@ def run_sweep_bench(args):
             table[s].box[k] = sy["L"]
         table[s].time_delta = SWEEP["dt"]
         table[s].skin = -1.0
+    # batch autotuner (skin x pair-kernel block size) on the sweep's own state; both
+    # arms then run with the chosen parameters, so their records stay comparable bit for bit
+    tune = nat.BatchTuning()
+    xs = np.concatenate([sy["x"] for sy in systems])
+    vs = np.concatenate([sy["v"] for sy in systems])
+    nat.check(lib.lj_batch_autotune(table, nsys, SWEEP["rc"], 0, P(xs), P(vs), 4, 200, ctypes.byref(tune)))
+    for s in range(nsys):
+        table[s].skin = tune.skin
+
+    # batched: one chunk-graph launch per 200-step chunk
     b = ctypes.c_void_p()
     nat.check(lib.lj_batch_create(table, nsys, SWEEP["rc"], 0, ctypes.byref(b)))
+    nat.check(lib.lj_batch_set_force_block(b, tune.force_block))
     for s, sy in enumerate(systems):
         nat.check(lib.lj_batch_upload_system(b, s, P(sy["x"]), P(sy["v"]), 4))
     recs = np.zeros((chunk, nsys, 7))
@@ -480,7 +490,8 @@ def run_sweep_bench(args):
     t0 = time.perf_counter()
     final_seq = np.zeros((nsys, 7))
     for s, sy in enumerate(systems):
-        with GpuSystem(sy["N"], sy["L"], cutoff=SWEEP["rc"], dt=SWEEP["dt"]) as g:
+        with GpuSystem(sy["N"], sy["L"], cutoff=SWEEP["rc"], dt=SWEEP["dt"], skin=tune.skin,
+                       force_block=tune.force_block) as g:
             g.upload(sy["x"], v=sy["v"])
             for step in range(0, total_steps, chunk):
                 r = g.step(chunk)
@@ -496,6 +507,8 @@ def run_sweep_bench(args):
             "speedup": t_seq / t_batched, "seconds_batched": t_batched, "seconds_sequential": t_seq,
             "systems": nsys, "atoms": atoms, "steps": total_steps,
             "identical_final_records": bool(np.array_equal(final_batched, final_seq)),
+            "tuning": {"skin": tune.skin, "force_block": tune.force_block,
+                       "tuned_ms_per_step": tune.ms_per_step, "source": "lj_batch_autotune, 200 steps per candidate"},
             "run_sweep_files": files,
             "config": {"workload": "8x8 grid rho in [0.05,1.0] x T in [0.5,2.0], N=4n^3, n~U{5..20} (seed 2024), "
                                    "rc=2.5, dt=0.005, 2000 equilibration + 5000 production steps, FP64",

@@ -391,8 +391,39 @@ int lj_batch_download_system(lj_batch* batch, int sys, double* x, double* v, dou
 /* An inactive system is frozen: its atoms are not integrated and it takes no steps. */
 int lj_batch_set_active(lj_batch* batch, int sys, int active);
 /* nsteps steps of every active system; out (may be NULL) receives nsteps x nsys
- * records, step-major (inactive systems' entries are not written). */
+ * records, step-major (inactive systems' entries are not written).  The steps
+ * run as one CUDA-graph launch per chunk of up to 256 steps: a device-side
+ * loop over 8-step bodies (each step's rebuild chain behind a conditional
+ * node), plus single launches for the last nsteps mod 8 steps.  The loop is
+ * bounded: a launch that reaches its iteration bound before its step count
+ * stops there and the call returns LJ_ERR_TIMEOUT (the systems are then short
+ * of the requested steps). */
 int lj_batch_step(lj_batch* batch, int nsteps, lj_thermo* out);
+/* Atoms per block of the batch's pair kernel: 64, 128 (the default) or 256.
+ * With the same block size (lj_params.force_block) and skin, a batched system
+ * evolves bit for bit as it does alone. */
+int lj_batch_set_force_block(lj_batch* batch, int force_block);
+
+/* Batch autotuner (the batched counterpart of lj_gpu_autotune): times `steps`
+ * steps of the whole batch for every candidate Verlet skin (0.2, 0.3, 0.4, 0.5,
+ * each clipped by the box as in lj_gpu_create) and pair-kernel block size (64,
+ * 128, 256), each in a fresh batch from the state x, v (every system's atoms
+ * in table order, stride doubles per atom; v may be NULL), and writes the
+ * fastest to *best.  The per-step work depends only on these two knobs: the
+ * list build's tiling (a warp per cell) and one atom per thread are fixed. */
+typedef struct lj_batch_tuning {
+    double skin;
+    int force_block;
+    double ms_per_step;
+} lj_batch_tuning;
+int lj_batch_autotune(const lj_batch_system* systems, int nsys, double cutoff, int device, const double* x,
+                      const double* v, int stride, int steps, lj_batch_tuning* best);
+
+/* The iteration bound of a chunk launch: 0 (the default) bounds it at the
+ * iterations the chunk needs; a positive limit overrides that, and a limit
+ * below a chunk's iterations makes its launch stop with LJ_ERR_TIMEOUT (the
+ * way the bound is tested). */
+int lj_batch_set_iteration_limit(lj_batch* batch, int limit);
 /* Instantaneous measurement of every system: out receives nsys records. */
 int lj_batch_measure(lj_batch* batch, lj_thermo* out);
 /* physics::set_temperature for one system (transformations.cpp:94-116). */

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstddef>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -37,7 +38,8 @@ namespace {
 struct SysDev {
     int atom_off, natoms;
     int cell_off, ncell;
-    int blk_off, nblk;
+    int blk_off, nblk;    // blocks of kThreads atoms (integration, measurement)
+    int fblk_off, nfblk;  // blocks of the pair kernel (force_block atoms)
     Grid grid;
     PairParams pp;
     double thresh2;  // rebuild when max |d - d_build|^2 exceeds this
@@ -60,6 +62,11 @@ struct BatchFlags {
     int overflow, nonfinite, any_rebuild, slot;  // slot: ring slot of the current step
     long long graph_rebuilds;
     long long step_count;                        // steps taken by the batch
+    // device-side loop of a chunk launch (set by the host before each launch)
+    int loop_left;         // body iterations still to run
+    int timeout;           // the loop hit loop_limit before loop_left reached 0
+    long long loop_iters;  // iterations run by this launch
+    long long loop_limit;  // upper bound on loop_iters
 };
 
 __device__ __forceinline__ bool sys_rebuild(const SysState* st, int s) { return st[s].rebuild != 0; }
@@ -118,6 +125,21 @@ static __global__ void b_decide_kernel(const SysDev* __restrict__ sys, SysState*
         if (any) fl->graph_rebuilds += 1;
         if (use_handle) cudaGraphSetConditional(h, any ? 1u : 0u);
     }
+}
+
+// End of one body iteration of a chunk launch: continue while iterations are
+// left.  The iteration count is bounded independently of loop_left: a launch
+// never runs more than loop_limit iterations, and one that would is stopped
+// with the timeout flag set (the host then returns LJ_ERR_TIMEOUT).
+static __global__ void b_loop_kernel(BatchFlags* fl, cudaGraphConditionalHandle h) {
+    int left = --fl->loop_left;
+    long long it = ++fl->loop_iters;
+    bool go = left > 0;
+    if (go && it >= fl->loop_limit) {
+        fl->timeout = 1;
+        go = false;
+    }
+    cudaGraphSetConditional(h, go ? 1u : 0u);
 }
 
 // ---- rebuild chain (systems with st[s].rebuild only) -------------------------
@@ -264,7 +286,8 @@ b_build_list_kernel(const int* __restrict__ cell_sys, const SysDev* __restrict__
 }
 
 // ---- pair force: per block one system, same loop as force_fp64_kernel ---------
-static __global__ void __launch_bounds__(kThreads, 4)
+template <int BS>
+static __global__ void __launch_bounds__(BS, 512 / BS)
 b_force_kernel(const int* __restrict__ blk_sys, const int* __restrict__ blk_first, const SysDev* __restrict__ sys,
                const SysState* st, int Ntot, const double4* __restrict__ pos, Soa s, const uint4* __restrict__ nbr4,
                const int* __restrict__ cnt, double* __restrict__ partials) {
@@ -315,12 +338,13 @@ b_force_kernel(const int* __restrict__ blk_sys, const int* __restrict__ blk_firs
             acc[3] = fma(d, d, acc[3]);
         }
     }
-    block_sum<4, kThreads>(acc);
+    block_sum<4, BS>(acc);
     if (threadIdx.x == 0)
         for (int q = 0; q < 4; ++q) partials[(size_t)blockIdx.x * 4 + q] = acc[q];
 }
 
-// One block per system: the single-system finalize over that system's blocks.
+// One block per system: the single-system finalize over that system's blocks
+// (after a step the pair kernel's blocks, after a measurement the kThreads ones).
 static __global__ void __launch_bounds__(1024)
 b_finalize_kernel(const SysDev* __restrict__ sys, SysState* st, int nsys, const double* __restrict__ partials,
                   double* __restrict__ ring, int ring_cap, int mode, BatchFlags* fl) {
@@ -329,9 +353,10 @@ b_finalize_kernel(const SysDev* __restrict__ sys, SysState* st, int nsys, const 
     SysState& T = st[sidx];
     if (mode == 0 && !T.active) return;
     double acc[4] = {0, 0, 0, 0};
-    for (int b = threadIdx.x; b < S.nblk; b += blockDim.x)
+    int off = mode == 2 ? S.blk_off : S.fblk_off, nb = mode == 2 ? S.nblk : S.nfblk;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) acc[q] += partials[(size_t)(S.blk_off + b) * 4 + q];
+        for (int q = 0; q < 4; ++q) acc[q] += partials[(size_t)(off + b) * 4 + q];
     block_sum<4, 1024>(acc);
     if (threadIdx.x == 0) {
         if (mode != 2) {
@@ -438,6 +463,8 @@ struct lj_batch {
     SysState* st = nullptr;
     BatchFlags* fl = nullptr;
     int *blk_sys = nullptr, *blk_first = nullptr, *sys_of = nullptr, *cell_sys = nullptr;
+    int force_block = kThreads, nfblk = 0;
+    int *fblk_sys = nullptr, *fblk_first = nullptr;  // pair-kernel block tables (room for 64-atom blocks)
     double4 *pos = nullptr, *pos_tmp = nullptr;
     float4* posf = nullptr;
     double *soa = nullptr, *soa_tmp = nullptr, *bd = nullptr, *partials = nullptr, *ring = nullptr;
@@ -451,6 +478,8 @@ struct lj_batch {
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
     bool graph_tried = false;
+    int loop_limit_override = 0;  // > 0: iteration bound of a chunk launch (testing the timeout path)
+    long long chunk_launches = 0;
     long long host_steps = 0;
     long long launches = 0;
     char err[512] = {0};
@@ -516,8 +545,13 @@ int launch_step_b(lj_batch* b, cudaGraphConditionalHandle* h) {
 
 int launch_force_b(lj_batch* b) {
     Soa s{b->soa, b->Ntot};
-    b_force_kernel<<<b->nblk, kThreads, 0, b->stream>>>(b->blk_sys, b->blk_first, b->sys, b->st, b->Ntot, b->pos, s,
-                                                        b->nbr, b->cnt, b->partials);
+#define LJ_BFORCE(BS)                                                                                          \
+    b_force_kernel<BS><<<b->nfblk, BS, 0, b->stream>>>(b->fblk_sys, b->fblk_first, b->sys, b->st, b->Ntot, b->pos, s, \
+                                                      b->nbr, b->cnt, b->partials)
+    if (b->force_block == 64) LJ_BFORCE(64);
+    else if (b->force_block == 256) LJ_BFORCE(256);
+    else LJ_BFORCE(128);
+#undef LJ_BFORCE
     BKL();
     b_finalize_kernel<<<b->nsys, 1024, 0, b->stream>>>(b->sys, b->st, b->nsys, b->partials, b->ring, b->ring_cap, 0,
                                                        b->fl);
@@ -536,12 +570,11 @@ int direct_step_b(lj_batch* b) {
 
 constexpr int kBatchGraphSteps = 8;
 
-int build_graph_b(lj_batch* b) {
+// Capture kBatchGraphSteps steps onto b->stream, which is capturing into some
+// graph: per step kick_drift -> decide -> IF(rebuild chain, captured on
+// b->side) -> force -> finalize.
+int capture_steps_b(lj_batch* b) {
     cudaStream_t main = b->stream;
-    long long l0 = b->launches;
-    cudaGraph_t graph = nullptr;
-    cudaError_t e = cudaStreamBeginCapture(main, cudaStreamCaptureModeThreadLocal);
-    if (e != cudaSuccess) return LJ_ERR_CUDA;
     int rc = LJ_OK;
     for (int k = 0; k < kBatchGraphSteps && rc == LJ_OK; ++k) {
         cudaStreamCaptureStatus cs;
@@ -581,12 +614,50 @@ int build_graph_b(lj_batch* b) {
         rc = launch_force_b(b);
     }
     b->stream = main;
-    e = cudaStreamEndCapture(main, &graph);
-    b->launches = l0;
-    if (rc == LJ_OK && e == cudaSuccess && cudaGraphInstantiate(&b->graph, graph, 0) == cudaSuccess) {
+    return rc;
+}
+
+// The chunk graph: one WHILE conditional node whose body is kBatchGraphSteps
+// steps followed by b_loop_kernel, so that one launch runs a whole chunk of
+// loop_left * kBatchGraphSteps steps with no host involvement (the loop
+// handle restarts at 1 on every launch: the body runs at least once).
+int build_graph_b(lj_batch* b) {
+    long long l0 = b->launches;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int rc = LJ_OK;
+    cudaGraphConditionalHandle hw;
+    cudaGraphNodeParams wp = {};
+    cudaGraphNode_t wn;
+    if (cudaGraphCreate(&graph, 0) != cudaSuccess ||
+        cudaGraphConditionalHandleCreate(&hw, graph, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
+        rc = LJ_ERR_CUDA;
+    } else {
+        wp.type = cudaGraphNodeTypeConditional;
+        wp.conditional.handle = hw;
+        wp.conditional.type = cudaGraphCondTypeWhile;
+        wp.conditional.size = 1;
+        if (cudaGraphAddNode(&wn, graph, nullptr, 0, &wp) != cudaSuccess ||
+            cudaStreamBeginCaptureToGraph(b->stream, wp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            rc = LJ_ERR_CUDA;
+        } else {
+            rc = capture_steps_b(b);
+            if (rc == LJ_OK) {
+                b_loop_kernel<<<1, 1, 0, b->stream>>>(b->fl, hw);
+                if (cudaGetLastError() != cudaSuccess) rc = LJ_ERR_CUDA;
+            }
+            cudaGraph_t body = nullptr;
+            if (cudaStreamEndCapture(b->stream, &body) != cudaSuccess && rc == LJ_OK) rc = LJ_ERR_CUDA;
+        }
+    }
+    b->launches = l0;  // captured launches are not executions
+    if (rc == LJ_OK && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+        b->graph = exec;
         b->graph_steps = kBatchGraphSteps;
     } else {
         b->graph = nullptr;
+        b->graph_steps = 0;
         rc = LJ_ERR_CUDA;
         cudaGetLastError();
     }
@@ -594,14 +665,27 @@ int build_graph_b(lj_batch* b) {
     return rc;
 }
 
+// Enqueue nsteps steps: one chunk-graph launch for the whole multiples of
+// kBatchGraphSteps (its loop count and bound set on the device first), single
+// launches for the rest.
 int enqueue_b(lj_batch* b, int nsteps) {
     if (!b->graph_tried) {
         b->graph_tried = true;
         build_graph_b(b);
     }
     int s = 0;
-    if (b->graph_steps > 0)
-        for (; s + b->graph_steps <= nsteps; s += b->graph_steps) BK(cudaGraphLaunch(b->graph, b->stream));
+    if (b->graph_steps > 0 && nsteps >= b->graph_steps) {
+        int iters = nsteps / b->graph_steps;
+        struct {
+            int loop_left, timeout;
+            long long loop_iters, loop_limit;
+        } ctl = {iters, 0, 0, b->loop_limit_override > 0 ? b->loop_limit_override : iters};
+        static_assert(sizeof ctl == sizeof(BatchFlags) - offsetof(BatchFlags, loop_left), "loop fields");
+        BK(cudaMemcpyAsync(&b->fl->loop_left, &ctl, sizeof ctl, cudaMemcpyHostToDevice, b->stream));
+        BK(cudaGraphLaunch(b->graph, b->stream));
+        ++b->chunk_launches;
+        s = iters * b->graph_steps;
+    }
     for (; s < nsteps; ++s) {
         int rc = direct_step_b(b);
         if (rc) return rc;
@@ -622,11 +706,21 @@ int read_flags_b(lj_batch* b) {
         std::snprintf(b->err, sizeof b->err, "non-finite energy or virial");
         return LJ_ERR_NONFINITE;
     }
+    if (h.timeout) {
+        // the launch took fewer steps than were enqueued: follow the device's
+        // step count (the ring slots) and clear the flag for the next call
+        b->host_steps = h.step_count;
+        BK(cudaMemsetAsync(&b->fl->timeout, 0, sizeof(int), b->stream));
+        BK(cudaStreamSynchronize(b->stream));
+        std::snprintf(b->err, sizeof b->err, "a chunk launch stopped at its iteration bound (%lld iterations)",
+                      h.loop_iters);
+        return LJ_ERR_TIMEOUT;
+    }
     return LJ_OK;
 }
 
 void free_b(lj_batch* b) {
-    void* ptrs[] = {b->sys, b->st, b->fl, b->blk_sys, b->blk_first, b->sys_of, b->cell_sys, b->pos, b->pos_tmp,
+    void* ptrs[] = {b->sys, b->st, b->fl, b->blk_sys, b->blk_first, b->fblk_sys, b->fblk_first, b->sys_of, b->cell_sys, b->pos, b->pos_tmp,
                     b->posf, b->soa, b->soa_tmp, b->bd, b->partials, b->ring, b->ids, b->ids_tmp, b->cell_of,
                     b->rank, b->order, b->count, b->start, b->cnt, b->nbr, b->dstats, b->natoms};
     for (void* p : ptrs)
@@ -635,6 +729,33 @@ void free_b(lj_batch* b) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
     if (b->side) cudaStreamDestroy(b->side);
     if (b->stream) cudaStreamDestroy(b->stream);
+}
+
+// Pair-kernel block tables for blocks of bs atoms (each block inside one
+// system, as the single-system pair kernel of that block size partitions it),
+// uploaded with the system table; the chunk graph is rebuilt on next use.
+int set_force_blocks(lj_batch* b, int bs) {
+    std::vector<int> fs, ff;
+    int off = 0;
+    for (SysDev& S : b->hsys) {
+        S.fblk_off = off;
+        S.nfblk = (S.natoms + bs - 1) / bs;
+        for (int j = 0; j < S.nfblk; ++j) {
+            fs.push_back((int)(&S - b->hsys.data()));
+            ff.push_back(S.atom_off + j * bs);
+        }
+        off += S.nfblk;
+    }
+    BK(cudaMemcpy(b->fblk_sys, fs.data(), sizeof(int) * fs.size(), cudaMemcpyHostToDevice));
+    BK(cudaMemcpy(b->fblk_first, ff.data(), sizeof(int) * ff.size(), cudaMemcpyHostToDevice));
+    BK(cudaMemcpy(b->sys, b->hsys.data(), sizeof(SysDev) * b->nsys, cudaMemcpyHostToDevice));
+    b->force_block = bs;
+    b->nfblk = off;
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+    b->graph_steps = 0;
+    b->graph_tried = false;
+    return LJ_OK;
 }
 
 }  // namespace
@@ -733,7 +854,11 @@ int lj_batch_create(const lj_batch_system* systems, int nsys, double cutoff, int
         BK(cudaMalloc(&b->soa, sizeof(double) * SOA_FIELDS * N));
         BK(cudaMalloc(&b->soa_tmp, sizeof(double) * SOA_FIELDS * N));
         BK(cudaMalloc(&b->bd, sizeof(double) * 3 * N));
-        BK(cudaMalloc(&b->partials, sizeof(double) * 4 * nblk));
+        long long nfblk64 = 0;
+        for (const SysDev& S : b->hsys) nfblk64 += (S.natoms + 63) / 64;
+        BK(cudaMalloc(&b->fblk_sys, sizeof(int) * nfblk64));
+        BK(cudaMalloc(&b->fblk_first, sizeof(int) * nfblk64));
+        BK(cudaMalloc(&b->partials, sizeof(double) * 4 * std::max<long long>(nblk, nfblk64)));
         BK(cudaMalloc(&b->ring, sizeof(double) * 7 * (size_t)(b->ring_cap + 1) * nsys));
         BK(cudaMallocHost(&b->host_ring, sizeof(double) * 7 * (size_t)(b->ring_cap + 1) * nsys));
         BK(cudaMalloc(&b->ids, sizeof(int) * N));
@@ -780,7 +905,7 @@ int lj_batch_create(const lj_batch_system* systems, int nsys, double cutoff, int
         BK(cudaMemcpy(b->ids, ident.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
         int sentinel = N;
         BK(cudaMemcpy(b->start + ncell, &sentinel, sizeof(int), cudaMemcpyHostToDevice));
-        return LJ_OK;
+        return set_force_blocks(b, kThreads);
     };
     if (int rc = init()) {
         cudaSetDevice(device);
@@ -926,6 +1051,19 @@ int lj_batch_set_temperature(lj_batch* b, int sys, double target, double* measur
     return LJ_OK;
 }
 
+int lj_batch_set_force_block(lj_batch* b, int force_block) {
+    if (!b || (force_block != 64 && force_block != 128 && force_block != 256)) return LJ_ERR_ARG;
+    BK(cudaSetDevice(b->device));
+    BK(cudaStreamSynchronize(b->stream));
+    return set_force_blocks(b, force_block);
+}
+
+int lj_batch_set_iteration_limit(lj_batch* b, int limit) {
+    if (!b || limit < 0) return LJ_ERR_ARG;
+    b->loop_limit_override = limit;
+    return LJ_OK;
+}
+
 int lj_batch_window_stats(lj_batch* b, int sample_size, const double* density, lj_observation* out) {
     if (!b || !density || !out || sample_size < 2 || sample_size > b->ring_cap || sample_size > b->host_steps)
         return LJ_ERR_ARG;
@@ -938,6 +1076,51 @@ int lj_batch_window_stats(lj_batch* b, int sample_size, const double* density, l
     static_assert(sizeof(lj_observation) == 6 * sizeof(double), "lj_observation is 6 doubles");
     BK(cudaMemcpyAsync(out, b->dstats, sizeof(double) * 6 * b->nsys, cudaMemcpyDeviceToHost, b->stream));
     BK(cudaStreamSynchronize(b->stream));
+    return LJ_OK;
+}
+
+// Batch autotuner: every candidate (Verlet skin of all systems x pair-kernel
+// block size) runs in a fresh batch from the caller's state -- 16 steps to
+// build the chunk graph and the first lists, then `steps` timed steps -- and
+// the fastest is returned.
+int lj_batch_autotune(const lj_batch_system* systems, int nsys, double cutoff, int device, const double* x,
+                      const double* v, int stride, int steps, lj_batch_tuning* best) {
+    if (!systems || nsys < 1 || !x || !best || steps < 8 || (stride != 3 && stride != 4)) return LJ_ERR_ARG;
+    const double skins[] = {0.2, 0.3, 0.4, 0.5};
+    const int blocks[] = {64, 128, 256};
+    std::vector<lj_batch_system> table(systems, systems + nsys);
+    lj_batch_tuning win{-1.0, 0, 1e300};
+    for (double sk : skins) {
+        for (lj_batch_system& q : table) q.skin = sk;
+        for (int bs : blocks) {
+            lj_batch* b = nullptr;
+            int rc = lj_batch_create(table.data(), nsys, cutoff, device, &b);
+            if (rc) return rc;
+            rc = lj_batch_set_force_block(b, bs);
+            size_t off = 0;
+            for (int s = 0; s < nsys && !rc; ++s) {
+                rc = lj_batch_upload_system(b, s, x + off, v ? v + off : nullptr, stride);
+                off += (size_t)stride * systems[s].particle_count;
+            }
+            if (!rc) rc = lj_batch_step(b, 16, nullptr);
+            cudaEvent_t e0 = nullptr, e1 = nullptr;
+            float ms = 0.f;
+            if (!rc && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)) rc = LJ_ERR_CUDA;
+            if (!rc) {
+                cudaEventRecord(e0, b->stream);
+                rc = lj_batch_step(b, steps, nullptr);
+                cudaEventRecord(e1, b->stream);
+            }
+            if (!rc && (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+                rc = LJ_ERR_CUDA;
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+            lj_batch_destroy(b);
+            if (rc) return rc;
+            if (ms / steps < win.ms_per_step) win = lj_batch_tuning{sk, bs, (double)ms / steps};
+        }
+    }
+    *best = win;
     return LJ_OK;
 }
 

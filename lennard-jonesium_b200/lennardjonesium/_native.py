@@ -104,6 +104,10 @@ class Observation(ctypes.Structure):
         "temperature", "density", "total_energy", "pressure", "specific_heat", "diffusion_coefficient")]
 
 
+class BatchTuning(ctypes.Structure):
+    _fields_ = [("skin", ctypes.c_double), ("force_block", ctypes.c_int), ("ms_per_step", ctypes.c_double)]
+
+
 class LJError(RuntimeError):
     """A C-ABI call returned a non-zero status."""
 
@@ -160,6 +164,10 @@ SIGNATURES = {
     "lj_batch_download_system": (ctypes.c_int, [P, ctypes.c_int, P, P, P, ctypes.c_int]),
     "lj_batch_set_active": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int]),
     "lj_batch_step": (ctypes.c_int, [P, ctypes.c_int, P]),
+    "lj_batch_set_iteration_limit": (ctypes.c_int, [P, ctypes.c_int]),
+    "lj_batch_set_force_block": (ctypes.c_int, [P, ctypes.c_int]),
+    "lj_batch_autotune": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double, ctypes.c_int, P, P, ctypes.c_int,
+                                         ctypes.c_int, P]),
     "lj_batch_measure": (ctypes.c_int, [P, P]),
     "lj_batch_set_temperature": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double, P]),
     "lj_batch_info": (ctypes.c_int, [P, P, P, P]),

@@ -107,7 +107,8 @@ _CTYPES = {"int": ctypes.c_int, "double": ctypes.c_double, "long long": ctypes.c
 @pytest.mark.parametrize("name,cls", [("lj_params", "Params"), ("lj_stats", "Stats"), ("lj_thermo", "Thermo"),
                                       ("lj_phase_times", "PhaseTimes"), ("lj_sim_config", "SimConfig"),
                                       ("lj_sim_result", "SimResult"), ("lj_batch_system", "BatchSystem"),
-                                      ("lj_adj_params", "AdjParams")])
+                                      ("lj_adj_params", "AdjParams"), ("lj_observation", "Observation"),
+                                      ("lj_batch_tuning", "BatchTuning")])
 def test_ctypes_structs_follow_the_header(name, cls):
     """The Python binding's structs list the header's fields in the header's order and types."""
     from lennardjonesium import _native

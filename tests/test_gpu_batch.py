@@ -25,9 +25,8 @@ SYSTEMS = [  # N, T, rho, seed: uneven sizes and densities (each box >= 3 cutoff
 ]
 
 
-def _batch(states, L):
+def _table(states, L, skin=-1.0):
     from lennardjonesium import _native as nat
-    lib = nat.lib()
     n = len(states)
     systems = (nat.BatchSystem * n)()
     for s, ((x, v), box) in enumerate(zip(states, L)):
@@ -35,9 +34,19 @@ def _batch(states, L):
         for k in range(3):
             systems[s].box[k] = box
         systems[s].time_delta = 0.005
-        systems[s].skin = -1.0
+        systems[s].skin = skin
+    return systems
+
+
+def _batch(states, L, skin=-1.0, force_block=0):
+    from lennardjonesium import _native as nat
+    lib = nat.lib()
+    n = len(states)
+    systems = _table(states, L, skin)
     b = ctypes.c_void_p()
     nat.check(lib.lj_batch_create(systems, n, 2.5, 0, ctypes.byref(b)))
+    if force_block:
+        nat.check(lib.lj_batch_set_force_block(b, force_block))
     for s, (x, v) in enumerate(states):
         nat.check(lib.lj_batch_upload_system(b, s, x.ctypes.data_as(ctypes.c_void_p),
                                              v.ctypes.data_as(ctypes.c_void_p), 4))
@@ -179,3 +188,69 @@ def test_context_window_statistics_on_device():
             want = _host_stats(recs[-W:], 4000, 0.8)
             assert np.all(np.abs(got - want) <= 1e-12 * np.abs(want)), (W, got, want)
         assert nat.lib().lj_gpu_window_stats(g._ctx, 1025, 0.8, ctypes.byref(o)) == nat.LJ_ERR_ARG
+
+
+def test_batch_chunk_loop_bound():
+    """A chunk launch runs its device-side loop under an iteration bound: with the
+    bound set below the chunk's 8 iterations the launch stops early and the call
+    returns LJ_ERR_TIMEOUT; with the default bound the same batch steps on, and
+    its records then equal a single-system run of the steps it really took."""
+    from lennardjonesium import GpuSystem
+    from lennardjonesium import _native as nat
+    N, T, rho, seed = SYSTEMS[1]
+    x, v, box = ljref.initial_state(N, T, rho, seed)
+    lib, b = _batch([(x, v)], [box])
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    try:
+        assert lib.lj_batch_set_iteration_limit(b, 3) == 0
+        assert lib.lj_batch_step(b, 64, None) == nat.LJ_ERR_TIMEOUT
+        assert b"iteration bound" in lib.lj_batch_last_error(b)
+        assert lib.lj_batch_set_iteration_limit(b, 0) == 0
+        assert lib.lj_batch_upload_system(b, 0, P(x), P(v), 4) == 0
+        recs = np.zeros((64, 1, 7))
+        assert lib.lj_batch_step(b, 64, P(recs)) == 0
+    finally:
+        lib.lj_batch_destroy(b)
+    with GpuSystem(N, box) as g:
+        g.upload(x, v=v)
+        ref = g.step(64)
+    assert np.array_equal(recs[:, 0, :], ref)
+
+
+@pytest.mark.parametrize("skin,block", [(0.4, 64), (0.2, 256)])
+def test_tuned_batch_equals_single_systems(skin, block):
+    """A batch run with another skin and pair-kernel block size (autotuner
+    candidates) equals single-system runs with the same parameters bit for bit."""
+    from lennardjonesium import GpuSystem
+    states, L = [], []
+    for N, T, rho, seed in SYSTEMS[:4]:
+        x, v, box = ljref.initial_state(N, T, rho, seed)
+        states.append((x, v))
+        L.append(box)
+    lib, b = _batch(states, L, skin=skin, force_block=block)
+    recs = np.zeros((90, len(states), 7))
+    try:
+        assert lib.lj_batch_step(b, 90, recs.ctypes.data_as(ctypes.c_void_p)) == 0
+    finally:
+        lib.lj_batch_destroy(b)
+    for s, ((x, v), box) in enumerate(zip(states, L)):
+        with GpuSystem(x.shape[0], box, skin=skin, force_block=block) as g:
+            g.upload(x, v=v)
+            ref = g.step(90)
+        assert np.array_equal(recs[:, s, :], ref), f"system {s}"
+
+
+def test_batch_autotune_returns_a_candidate():
+    from lennardjonesium import _native as nat
+    states, L = [], []
+    for N, T, rho, seed in SYSTEMS[:3]:
+        x, v, box = ljref.initial_state(N, T, rho, seed)
+        states.append((x, v))
+        L.append(box)
+    x = np.concatenate([a for a, _ in states])
+    v = np.concatenate([b for _, b in states])
+    best = nat.BatchTuning()
+    rc = nat.lib().lj_batch_autotune(_table(states, L), len(states), 2.5, 0, x.ctypes.data_as(ctypes.c_void_p),
+                                     v.ctypes.data_as(ctypes.c_void_p), 4, 16, ctypes.byref(best))
+    assert rc == 0
+    assert best.skin in (0.2, 0.3, 0.4, 0.5) and best.force_block in (64, 128, 256) and best.ms_per_step > 0
