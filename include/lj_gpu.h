@@ -72,17 +72,9 @@ typedef struct lj_params {
     double skin;             /* Verlet-list skin; < 0 selects the default (0.3) */
     int neighbor_capacity;   /* list entries per atom; 0 selects a density-based default */
     int force_block;         /* atoms per block of the pair kernel: 64, 128 or 256; 0 selects 128 */
-    /* Mixed path only: 0 runs the pair kernel as a neighbour-list gather
-     * from global memory; 1..8 runs it over shared-memory tiles of that many
-     * consecutive list cells of one column.  tile_capacity: the window atoms
-     * a tile stages in shared memory (0 selects a density-based default; a
-     * tile whose window holds more reads from global memory). */
-    int tile_cells;
-    int tile_capacity;
-    /* Mixed path, neighbour-list kernel: 0 adds FP32 sums of 8 consecutive
-     * pair forces (and V, W) into the FP64 per-atom accumulators; 1 adds every
-     * pair's FP32 force, V and W in FP64 (no FP32 summation; slower).  Must be
-     * 0 with tile_cells > 0. */
+    /* Mixed path: 0 adds FP32 sums of 8 consecutive pair forces (and V, W)
+     * into the FP64 per-atom accumulators; 1 adds every pair's FP32 force, V
+     * and W in FP64 (no FP32 summation; slower). */
     int mixed_per_pair;
 } lj_params;
 
@@ -120,9 +112,6 @@ typedef struct lj_stats {
     int small_box;             /* 1: explicit lattice images, rebuilt every step */
     double skin;               /* skin in use (0 in small-box mode) */
     long long kernel_launches; /* kernels this context has launched */
-    int tile_cells;            /* mixed path: cells per shared-memory tile (0: no tiles) */
-    int tile_capacity;         /* mixed path: window atoms one tile stages */
-    int max_staged;            /* mixed path: largest tile window at the last build */
 } lj_stats;
 
 typedef struct lj_ctx lj_ctx;
@@ -257,8 +246,7 @@ int lj_gpu_step_timed(lj_ctx* ctx, int nsteps, lj_phase_times* out);
 /* Project autotuner: times `steps` steps of the system described by base and
  * the state (x, v; N x stride doubles) for each candidate skin (the list-cell
  * edge rc + skin and the rebuild frequency) and pair-kernel block size (atoms
- * per block: 64, 128, 256) -- on the mixed path also the shared-memory tile
- * kernel at 3 or 6 cells per tile -- each in a fresh context from the same
+ * per block: 64, 128, 256), each in a fresh context from the same
  * state, and writes the fastest parameters to *best (and its ms per step). */
 int lj_gpu_autotune(const lj_params* base, const double* x, const double* v, int stride, int steps,
                     lj_params* best, double* best_ms_per_step);

@@ -16,8 +16,6 @@ cdef extern from "lj_gpu.h":
         double skin
         int neighbor_capacity
         int force_block
-        int tile_cells
-        int tile_capacity
         int mixed_per_pair
     ctypedef struct lj_thermo:
         double time

@@ -42,7 +42,6 @@ struct Scalars {
     long long builds;              // neighbour-list builds so far
     long long steps;
     long long graph_rebuilds;      // rebuild subgraphs executed by step graphs
-    int max_staged;                // mixed path: largest tile window at the last build
 };
 
 // Physical constants of the pair kernel.

@@ -26,7 +26,6 @@
 #include "../../include/lj_gpu.h"
 #include "lj_kernels.cuh"
 #include "lj_mixed.cuh"
-#include "lj_tile.cuh"
 
 using namespace ljb;
 
@@ -88,13 +87,6 @@ struct lj_ctx {
     // mixed-precision buffers
     float4* posl = nullptr;
     double* bx = nullptr;  // x at build (unwrapped reference for local coordinates)
-    // shared-memory tiles of the mixed pair kernel (lj_tile.cuh)
-    bool tiles = false;
-    TileGeom tg{};
-    int tile_cells = 0;
-    int tile_blocks = 0;
-    size_t tile_smem = 0;
-    uint4* nbr8 = nullptr;  // 16-bit tile entries, groups of 8
 
     // debug (reference grid) buffers, allocated on first use
     int* dbg_count = nullptr;
@@ -209,7 +201,7 @@ int launch_binning(lj_ctx* ctx, const Grid& g, int* count, int* start, int* tile
 
 // Rebuild chain: bin into the list grid, sort, gather, list.  Every kernel
 // returns at once when the gate is closed.
-int launch_rebuild(lj_ctx* ctx, bool tile_format = true) {
+int launch_rebuild(lj_ctx* ctx) {
     Gate gate = gate_of(ctx);
     int N = ctx->N;
     int rc = launch_binning<true>(ctx, ctx->list_grid, ctx->count, ctx->start, ctx->tile_sums, gate);
@@ -237,10 +229,6 @@ int launch_rebuild(lj_ctx* ctx, bool tile_format = true) {
     if (ctx->small_box)
         build_list_kernel<true><<<blocks_for(N), kThreads, 0, ctx->stream>>>(
             N, ctx->pos, ctx->posf, ctx->list_grid, ctx->start, Lf, cut2, ctx->cap, ctx->nbr, ctx->cnt, ctx->sc, gate);
-    else if (ctx->tiles && tile_format)
-        build_list_tile_kernel<<<blocks_for(ctx->list_grid.ncell(), kBuildWarps), 32 * kBuildWarps, 0, ctx->stream>>>(
-            N, ctx->posf, ctx->list_grid, ctx->start, Lf, cut2, ctx->cap, ctx->tg.nruns, ctx->nbr8, ctx->cnt, ctx->sc,
-            gate);
     else
         build_list_warp_kernel<<<blocks_for(ctx->list_grid.ncell(), kBuildWarps), 32 * kBuildWarps, 0, ctx->stream>>>(
             N, ctx->pos, ctx->posf, ctx->list_grid, ctx->start, Lf, cut2, ctx->cap, ctx->nbr, ctx->cnt, ctx->sc, gate);
@@ -259,17 +247,6 @@ int launch_force_bs(lj_ctx* ctx, bool kick, const Fuse& fz) {
     Soa s = soa_of(ctx->soa, N);
     dim3 gr(ctx->fblocks), bl(BS);
     int kind = ctx->p.force_kind;
-    if (ctx->tiles) {
-        MixedParams mp = mixed_params(ctx->pp, ctx->list_grid);
-        if (kick)
-            force_mixed_tile_kernel<true><<<ctx->tile_blocks, kTileThreads, ctx->tile_smem, ctx->stream>>>(
-                N, ctx->posl, s, ctx->nbr8, ctx->cnt, ctx->start, ctx->list_grid, ctx->tg, ctx->pp, mp, ctx->partials);
-        else
-            force_mixed_tile_kernel<false><<<ctx->tile_blocks, kTileThreads, ctx->tile_smem, ctx->stream>>>(
-                N, ctx->posl, s, ctx->nbr8, ctx->cnt, ctx->start, ctx->list_grid, ctx->tg, ctx->pp, mp, ctx->partials);
-        CKL();
-        return LJ_OK;
-    }
     if (ctx->p.precision == LJ_PRECISION_MIXED && kind == LJ_FORCE_LJ && !ctx->small_box) {
         MixedParams mp = mixed_params(ctx->pp, ctx->list_grid);
 #define LJ_MIXED_LAUNCH(KK, PP)                                                                          \
@@ -300,9 +277,9 @@ int launch_force_bs(lj_ctx* ctx, bool kick, const Fuse& fz) {
     return LJ_OK;
 }
 
-// Whether a pair kernel can carry the next step's kick and drift (the
-// neighbour-list kernels with a second kick; not the shared-memory tiles).
-bool can_fuse(const lj_ctx* ctx) { return ctx->p.force_kind != LJ_FORCE_NONE && !ctx->tiles; }
+// Whether a pair kernel can carry the next step's kick and drift (every
+// configuration with a force calculation).
+bool can_fuse(const lj_ctx* ctx) { return ctx->p.force_kind != LJ_FORCE_NONE; }
 
 // Pair kernel at the context's block size (64, 128 or 256 atoms per block).
 // With pos_next / posl_next it also runs the next step's first half kick and
@@ -329,7 +306,7 @@ int launch_force(lj_ctx* ctx, bool kick, double4* pos_next = nullptr, float4* po
 
 // Number of partial-sum blocks the last step's measurement pass wrote.
 int partial_blocks(const lj_ctx* ctx, bool forces) {
-    return forces ? (ctx->tiles ? ctx->tile_blocks : ctx->fblocks) : ctx->nblocks;
+    return forces ? ctx->fblocks : ctx->nblocks;
 }
 
 int launch_kick_drift(lj_ctx* ctx, double4* pos_out = nullptr, float4* posl_out = nullptr) {
@@ -709,7 +686,7 @@ int read_flags(lj_ctx* ctx) {
 void free_all(lj_ctx* c) {
     void* ptrs[] = {c->posf, c->pos, c->pos_tmp, c->soa, c->soa_tmp, c->bd, c->ids, c->ids_tmp, c->cell_of,
                     c->rank, c->order, c->count, c->start, c->tile_sums, c->nbr, c->cnt, c->partials,
-                    c->sc, c->ring, c->dscratch, c->dstats, c->posl, c->bx, c->nbr8, c->pos_b, c->posl_b, c->dbg_count,
+                    c->sc, c->ring, c->dscratch, c->dstats, c->posl, c->bx, c->pos_b, c->posl_b, c->dbg_count,
                     c->dbg_start,
                     c->dbg_members, c->dbg_cell_of, c->dbg_tiles};
     for (void* q : ptrs)
@@ -772,7 +749,7 @@ int init_ctx(lj_ctx* ctx, const lj_params& p) {
     double expect = 4.0 / 3.0 * M_PI * cut * cut * cut * std::max(rho, 1.2);
     int cap = p.neighbor_capacity > 0 ? p.neighbor_capacity : (int)std::ceil(1.5 * expect + 32);
     cap = std::min(cap, std::max(N - 1, 1) * 27);
-    cap = (std::max(cap, 1) + 7) & ~7;  // whole groups of 4 (FP64 list) and of 8 (tile list)
+    cap = (std::max(cap, 1) + 3) & ~3;  // whole groups of 4 entries
     ctx->cap = cap;
     ctx->nblocks = blocks_for(N);
     if (p.force_block != 0 && p.force_block != 64 && p.force_block != 128 && p.force_block != 256) {
@@ -780,31 +757,6 @@ int init_ctx(lj_ctx* ctx, const lj_params& p) {
     }
     ctx->force_block = p.force_block ? p.force_block : 128;
     ctx->fblocks = blocks_for(N, ctx->force_block);
-    if (p.tile_cells < 0 || p.tile_cells > kTileMaxRun || p.tile_capacity < 0 || p.tile_capacity > kTileMaxSmemAtoms) {
-        return LJ_ERR_ARG;
-    }
-    // mixed path over shared-memory tiles: runs of tile_cells list cells per
-    // column (a run plus its two neighbour cells must not wrap onto itself)
-    if (p.precision == LJ_PRECISION_MIXED && p.force_kind == LJ_FORCE_LJ && !ctx->small_box && p.tile_cells > 0) {
-        const Grid& g = ctx->list_grid;
-        int want = p.tile_cells;
-        int nruns = std::max(1, (g.n[2] + want - 1) / want);
-        while ((g.n[2] + nruns - 1) / nruns + 2 > g.n[2]) ++nruns;
-        int run_max = (g.n[2] + nruns - 1) / nruns;
-        double a3 = (p.box[0] / g.n[0]) * (p.box[1] / g.n[1]) * (p.box[2] / g.n[2]);
-        double expect_win = 9.0 * (run_max + 2) * std::max(rho, 0.1) * a3;
-        int tcap = p.tile_capacity ? p.tile_capacity : (int)std::ceil(1.5 * expect_win + 128);
-        tcap = std::min(kTileMaxSmemAtoms, (tcap + 127) & ~127);
-        if (p.tile_capacity) tcap = p.tile_capacity;
-        ctx->tiles = true;
-        ctx->tile_cells = (g.n[2] + nruns - 1) / nruns;
-        ctx->tg.nruns = nruns;
-        ctx->tg.cap = tcap;
-        for (int k = 0; k < 3; ++k) ctx->tg.a[k] = (float)(p.box[k] / g.n[k]);
-        ctx->tile_blocks = g.n[0] * g.n[1] * nruns;
-        ctx->tile_smem = sizeof(float4) * (size_t)(tcap + 1);
-    }
-
     int ncl = ctx->list_grid.ncell();
     // slot N is a ghost far outside the box: it pads the last neighbour group
     CK(cudaMalloc(&ctx->pos, sizeof(double4) * (N + 1)));
@@ -824,13 +776,7 @@ int init_ctx(lj_ctx* ctx, const lj_params& p) {
     CK(cudaMalloc(&ctx->tile_sums, sizeof(int) * kMaxScanTiles));
     CK(cudaMalloc(&ctx->nbr, sizeof(uint4) * (size_t)(cap / 4) * N));
     CK(cudaMalloc(&ctx->cnt, sizeof(int) * N));
-    CK(cudaMalloc(&ctx->partials, sizeof(double) * 4 * std::max(std::max(ctx->nblocks, ctx->fblocks), ctx->tile_blocks)));
-    if (ctx->tiles) {
-        CK(cudaMalloc(&ctx->nbr8, sizeof(uint4) * (size_t)(cap / 8) * N));
-        int smem = (int)ctx->tile_smem;
-        CK(cudaFuncSetAttribute(force_mixed_tile_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        CK(cudaFuncSetAttribute(force_mixed_tile_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    }
+    CK(cudaMalloc(&ctx->partials, sizeof(double) * 4 * std::max(ctx->nblocks, ctx->fblocks)));
     CK(cudaMalloc(&ctx->sc, sizeof(Scalars)));
     ctx->ring_cap = 1024;
     CK(cudaMalloc(&ctx->ring, sizeof(double) * 7 * (ctx->ring_cap + 1)));
@@ -927,9 +873,8 @@ int lj_gpu_create(const lj_params* params, lj_ctx** out) {
     if (p.force_kind < LJ_FORCE_NONE || p.force_kind > LJ_FORCE_CONSTANT) return LJ_ERR_ARG;
     if (p.precision != LJ_PRECISION_FP64 && p.precision != LJ_PRECISION_MIXED) return LJ_ERR_ARG;
     if (!p.periodic && p.force_kind != LJ_FORCE_NONE) return LJ_ERR_ARG;
-    // per-pair FP64 sums exist for the neighbour-list mixed kernel, not the tiles
     if (p.mixed_per_pair != 0 && p.mixed_per_pair != 1) return LJ_ERR_ARG;
-    if (p.mixed_per_pair && p.tile_cells > 0) return LJ_ERR_ARG;
+    if (p.force_block != 0 && p.force_block != 64 && p.force_block != 128 && p.force_block != 256) return LJ_ERR_ARG;
     // lennard_jones_force.cpp:45 -- the cutoff must lie beyond the potential minimum
     if (p.force_kind == LJ_FORCE_LJ && !(p.cutoff_distance * p.cutoff_distance > std::cbrt(2.0)))
         return LJ_ERR_ARG;
@@ -1153,11 +1098,8 @@ long long lj_gpu_debug_pairs(lj_ctx* ctx, long long cap, int* pi, int* pj, int* 
     int one = 1;
     if (cudaMemcpyAsync(&ctx->sc->need_rebuild, &one, sizeof(int), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
         return -LJ_ERR_CUDA;
-    int rc = launch_rebuild(ctx, false);  // the slot-indexed list, whatever the pair kernel reads
+    int rc = launch_rebuild(ctx);
     if (rc) return -rc;
-    if (ctx->tiles &&  // the tiled kernel's list is now stale: rebuild it before the next step
-        cudaMemcpyAsync(&ctx->sc->need_rebuild, &one, sizeof(int), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
-        return -LJ_ERR_CUDA;
     int* di = nullptr; int* dj = nullptr; int* dm = nullptr; double* dr = nullptr;
     unsigned long long* counter = nullptr;
     long long c = cap > 0 ? cap : 1;
@@ -1215,9 +1157,6 @@ int lj_gpu_get_stats(const lj_ctx* ctx_c, lj_stats* out) {
     // kernels, and the rebuild chain each time a conditional opened)
     out->kernel_launches = ctx->launches + (long long)ctx->rebuild_kernels * h.graph_rebuilds;
     for (const StepGraph& g : ctx->graphs) out->kernel_launches += g.launches * g.kernels;
-    out->tile_cells = ctx->tiles ? ctx->tile_cells : 0;
-    out->tile_capacity = ctx->tiles ? ctx->tg.cap : 0;
-    out->max_staged = h.max_staged;
     return LJ_OK;
 }
 
@@ -1426,10 +1365,8 @@ int lj_gpu_trajectory_close(lj_ctx* ctx, long long* frames) {
 // Project autotuner: for the caller's system (base params + state), time
 // `steps` velocity-Verlet steps for every candidate and return the fastest
 // parameters.  Candidates: the Verlet skin, which sets the list-cell edge
-// rc + skin and, against it, the rebuild frequency; and per skin either the
-// pair kernel's block size (atoms per block: 64, 128, 256) and, on the mixed
-// path (chunked FP32 pair sums), also its shared-memory tile variant at 3 or
-// 6 cells per tile.
+// rc + skin and, against it, the rebuild frequency; and per skin the pair
+// kernel's block size (atoms per block: 64, 128, 256).
 // Each candidate runs in its own context from the same initial state after a
 // warm-up long enough to build the step graph and the first neighbour list.
 int lj_gpu_autotune(const lj_params* base, const double* x, const double* v, int stride, int steps,
@@ -1437,7 +1374,6 @@ int lj_gpu_autotune(const lj_params* base, const double* x, const double* v, int
     if (!base || !x || !best || steps < 1 || (stride != 3 && stride != 4)) return LJ_ERR_ARG;
     const double skins[] = {0.15, 0.2, 0.3, 0.4, 0.5};
     const int blocks[] = {64, 128, 256};
-    const int tile_shapes[] = {3, 6};
     double best_ms = 1e300;
     lj_params winner = *base;
     double Lmin = std::min(base->box[0], std::min(base->box[1], base->box[2]));
@@ -1446,18 +1382,10 @@ int lj_gpu_autotune(const lj_params* base, const double* x, const double* v, int
         double eff = list_skin(sk, Lmin, base->cutoff_distance);
         if (eff == last_skin) continue;  // the box clips this skin to one already tried
         last_skin = eff;
-        Grid lg = make_grid(base->box, base->cutoff_distance + eff);
-        bool tiled = base->precision == LJ_PRECISION_MIXED && base->force_kind == LJ_FORCE_LJ &&
-                     !base->mixed_per_pair && std::min(lg.n[0], std::min(lg.n[1], lg.n[2])) >= 3;
-        for (int q = 0; q < (tiled ? 5 : 3); ++q) {
+        for (int bs : blocks) {
             lj_params p = *base;
             p.skin = sk;
-            if (q < 3) {
-                p.force_block = blocks[q];
-                p.tile_cells = 0;
-            } else {
-                p.tile_cells = tile_shapes[q - 3];
-            }
+            p.force_block = bs;
             lj_ctx* ctx = nullptr;
             int rc = lj_gpu_create(&p, &ctx);
             if (rc) return rc;

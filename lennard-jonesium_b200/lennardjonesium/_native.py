@@ -30,8 +30,6 @@ class Params(ctypes.Structure):
         ("skin", ctypes.c_double),
         ("neighbor_capacity", ctypes.c_int),
         ("force_block", ctypes.c_int),
-        ("tile_cells", ctypes.c_int),
-        ("tile_capacity", ctypes.c_int),
         ("mixed_per_pair", ctypes.c_int),
     ]
 
@@ -52,9 +50,6 @@ class Stats(ctypes.Structure):
         ("small_box", ctypes.c_int),
         ("skin", ctypes.c_double),
         ("kernel_launches", ctypes.c_longlong),
-        ("tile_cells", ctypes.c_int),
-        ("tile_capacity", ctypes.c_int),
-        ("max_staged", ctypes.c_int),
     ]
 
 

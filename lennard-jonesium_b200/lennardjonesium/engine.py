@@ -51,21 +51,20 @@ def initial_condition(N, temperature, density, seed):
 
 
 def autotune(N, box, x, v, steps=100, **kw):
-    """Project autotuner (lj_gpu_autotune): the fastest (skin, force_block) -- or,
-    on the mixed path's shared-memory tiles, (skin, tile_cells) -- for this
-    system and state, as GpuSystem keyword arguments, plus its ms per step."""
+    """Project autotuner (lj_gpu_autotune): the fastest (skin, force_block) for
+    this system and state, as GpuSystem keyword arguments, plus its ms per step."""
     base = _params(N, box, **kw)
     best = nat.Params()
     ms = ctypes.c_double()
     xs, vs = _as4(x, N), _as4(v, N) if v is not None else None
     nat.check(nat.lib().lj_gpu_autotune(ctypes.byref(base), _p(xs), _p(vs), 4, int(steps), ctypes.byref(best),
                                         ctypes.byref(ms)))
-    return {"skin": best.skin, "force_block": best.force_block, "tile_cells": best.tile_cells,
+    return {"skin": best.skin, "force_block": best.force_block,
             "mixed_per_pair": bool(best.mixed_per_pair)}, ms.value
 
 
 def _params(N, box, cutoff=2.5, dt=0.005, precision="fp64", force="lj", strength=0.0, periodic=True, device=0,
-            skin=None, capacity=0, force_block=0, tile_cells=0, tile_capacity=0, mixed_per_pair=False):
+            skin=None, capacity=0, force_block=0, mixed_per_pair=False):
     L = nat.lib()
     p = nat.Params()
     L.lj_gpu_default_params(ctypes.byref(p))
@@ -83,8 +82,6 @@ def _params(N, box, cutoff=2.5, dt=0.005, precision="fp64", force="lj", strength
     p.skin = -1.0 if skin is None else float(skin)
     p.neighbor_capacity = int(capacity)
     p.force_block = int(force_block)
-    p.tile_cells = int(tile_cells)
-    p.tile_capacity = int(tile_capacity)
     p.mixed_per_pair = 1 if mixed_per_pair else 0
     return p
 
@@ -98,17 +95,15 @@ class GpuSystem:
     (the reference's test mock, with `strength`) or "none".  skin: Verlet skin
     (None: 0.3); capacity: list entries per atom (0: density-based);
     force_block: atoms per pair-kernel block (64, 128, 256; 0: 128).  Mixed path
-    only: tile_cells / tile_capacity select the shared-memory tile kernel, and
-    mixed_per_pair adds every pair force in FP64 instead of FP32 sums of 8
-    pairs.  Every call raises LJError on a non-zero status."""
+    only: mixed_per_pair adds every pair force in FP64 instead of FP32 sums of
+    8 pairs.  Every call raises LJError on a non-zero status."""
 
     def __init__(self, N, box, cutoff=2.5, dt=0.005, precision="fp64", force="lj", strength=0.0,
-                 periodic=True, device=0, skin=None, capacity=0, force_block=0, tile_cells=0, tile_capacity=0,
-                 mixed_per_pair=False):
+                 periodic=True, device=0, skin=None, capacity=0, force_block=0, mixed_per_pair=False):
         L = nat.lib()
         p = _params(N, box, cutoff=cutoff, dt=dt, precision=precision, force=force, strength=strength,
                     periodic=periodic, device=device, skin=skin, capacity=capacity, force_block=force_block,
-                    tile_cells=tile_cells, tile_capacity=tile_capacity, mixed_per_pair=mixed_per_pair)
+                    mixed_per_pair=mixed_per_pair)
         b = np.broadcast_to(np.asarray(box, dtype=np.float64), (3,))
         self.N = int(N)
         self.box = b.copy()

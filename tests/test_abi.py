@@ -68,7 +68,7 @@ def test_create_rejects_bad_arguments():
     p.periodic = 1
     p.mixed_per_pair = 2  # a flag: 0 or 1
     assert L.lj_gpu_create(ctypes.byref(p), ctypes.byref(ctx)) == _native.LJ_ERR_ARG
-    p.mixed_per_pair, p.tile_cells = 1, 3  # per-pair FP64 sums are not built for the tiles
+    p.mixed_per_pair, p.force_block = 0, 96  # block sizes 64, 128, 256
     assert L.lj_gpu_create(ctypes.byref(p), ctypes.byref(ctx)) == _native.LJ_ERR_ARG
 
 

@@ -443,3 +443,29 @@ def test_autotune_returns_a_candidate():
     x, v, L = ljref.initial_state(4000, 1.2, 0.8, 7)
     kw, ms = autotune(4000, L, x, v, steps=24)
     assert kw["force_block"] in (64, 128, 256) and 0.0 <= kw["skin"] <= 0.5 and ms > 0
+
+
+@pytest.mark.parametrize("per_pair", [False, True])
+def test_mixed_full_size_force_error(per_pair):
+    """N = 1 048 576 (4 * 64^3 FCC, rho = 0.8442, perturbed): the mixed forces
+    against the FP64 path (itself at 1e-12 of the oracle), both accumulation modes."""
+    from lennardjonesium import initial_condition
+    N = 4 * 64 ** 3
+    x, v, L = initial_condition(N, 1.0, 0.8442, 5489)
+    rng = np.random.default_rng(5489)
+    x[:, :3] = np.mod(x[:, :3] + 0.08 * rng.standard_normal((N, 3)), L)
+    with gpu_system(N, L) as g:
+        g.upload(x)
+        pe64, w64 = g.compute_forces()
+        F64 = g.download()["F"]
+    with gpu_system(N, L, precision="mixed", mixed_per_pair=per_pair) as g:
+        g.upload(x)
+        pe32, w32 = g.compute_forces()
+        F32 = g.download()["F"]
+    S = ljref.force_abs_sum(x, L, 2.5)
+    err = np.sqrt(np.sum((F32 - F64)[:, :3] ** 2, axis=1))
+    assert np.all(err <= 1e-5 * S)
+    rms = np.sqrt(np.mean(np.sum(F64[:, :3] ** 2, axis=1)))
+    assert np.sqrt(np.mean(err ** 2)) / rms < 2e-5
+    assert abs(pe32 - pe64) / abs(pe64) < 1e-6
+    assert abs(w32 - w64) / abs(w64) < 1e-5
