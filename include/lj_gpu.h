@@ -244,8 +244,9 @@ typedef struct lj_phase_times {
 int lj_gpu_step_timed(lj_ctx* ctx, int nsteps, lj_phase_times* out);
 
 /* Project autotuner: times `steps` steps of the system described by base and
- * the state (x, v; N x stride doubles) for each candidate skin (the list-cell
- * edge rc + skin and the rebuild frequency) and pair-kernel block size (atoms
+ * the state (x, v; N x stride doubles) for each candidate skin (0.15 to 0.7;
+ * it sets the list-cell edge rc + skin and the rebuild frequency) and
+ * pair-kernel block size (atoms
  * per block: 64, 128, 256), each in a fresh context from the same
  * state, and writes the fastest parameters to *best (and its ms per step). */
 int lj_gpu_autotune(const lj_params* base, const double* x, const double* v, int stride, int steps,

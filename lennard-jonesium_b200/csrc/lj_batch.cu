@@ -301,7 +301,7 @@ b_force_kernel(const int* __restrict__ blk_sys, const int* __restrict__ blk_firs
         const double4 xi = pos[i];
         bool near = !(xi.x >= pp.near_lo && xi.x < pp.near_hi[0] && xi.y >= pp.near_lo &&
                       xi.y < pp.near_hi[1] && xi.z >= pp.near_lo && xi.z < pp.near_hi[2]);
-        double fx = 0, fy = 0, fz = 0, pe = 0, w = 0;
+        LjSums a;
         int ng = (cnt[i] + 3) >> 2;
         uint4 cur = ng > 0 ? __ldcs(&nbr4[i]) : make_uint4(0, 0, 0, 0);
         for (int g = 0; g < ng; ++g) {
@@ -312,23 +312,17 @@ b_force_kernel(const int* __restrict__ blk_sys, const int* __restrict__ blk_firs
             for (int u = 0; u < 4; ++u) q[u] = ld_pos(pos + entry_slot(e[u]));
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                double dx, dy, dz, f, V, W;
+                double dx, dy, dz;
                 separation<false>(xi, q[u], e[u], near, pp, dx, dy, dz);
-                pair_fp64<KIND_LJ>(pp, norm2(dx, dy, dz), f, V, W);
-                fx = fma(f, dx, fx);
-                fy = fma(f, dy, fy);
-                fz = fma(f, dz, fz);
-                pe += V;
-                w += W;
+                lj_accumulate(pp, dx, dy, dz, a);
             }
             cur = nxt;
         }
-        s.at(FX, i) = fx;
-        s.at(FY, i) = fy;
-        s.at(FZ, i) = fz;
-        acc[1] = pe;
-        acc[2] = w;
-        double f3[3] = {fx, fy, fz};
+        s.at(FX, i) = a.fx;
+        s.at(FY, i) = a.fy;
+        s.at(FZ, i) = a.fz;
+        lj_energy(pp, a, acc[1], acc[2]);
+        double f3[3] = {a.fx, a.fy, a.fz};
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             double v = kick(s.at(VX + k, i), f3[k], pp.dt);

@@ -1372,7 +1372,7 @@ int lj_gpu_trajectory_close(lj_ctx* ctx, long long* frames) {
 int lj_gpu_autotune(const lj_params* base, const double* x, const double* v, int stride, int steps,
                     lj_params* best, double* best_ms_per_step) {
     if (!base || !x || !best || steps < 1 || (stride != 3 && stride != 4)) return LJ_ERR_ARG;
-    const double skins[] = {0.15, 0.2, 0.3, 0.4, 0.5};
+    const double skins[] = {0.15, 0.2, 0.3, 0.4, 0.5, 0.6, 0.7};
     const int blocks[] = {64, 128, 256};
     double best_ms = 1e300;
     lj_params winner = *base;

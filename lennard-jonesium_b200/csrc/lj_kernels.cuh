@@ -652,6 +652,43 @@ __device__ __forceinline__ void pair_fp64(const PairParams& pp, double r2, doubl
     }
 }
 
+// LJ spline pairs of one atom (lennard_jones_force.cpp:107-119) accumulated as
+// the force plus power sums: with u = r^-6 and x = r^2 / rc^2 the pair terms
+// are V = 4u(u - 1) + beta x + (alpha - beta) and W = u(48u - 24) - 2 beta x,
+// so the atom's energy and virial follow from sum u^2, sum u, sum r^2 and the
+// pair count, formed once per atom, instead of V and W per pair (23 instead of
+// 28 FP64 operations per pair).  Pairs at or beyond the cutoff add nothing.
+struct LjSums {
+    double fx = 0, fy = 0, fz = 0, su2 = 0, su = 0, sr2 = 0;
+    int nh = 0;
+};
+
+__device__ __forceinline__ void lj_accumulate(const PairParams& pp, double dx, double dy, double dz, LjSums& a) {
+    const double wq = -2.0 * pp.beta * pp.inv_rc2;
+    double r2 = norm2(dx, dy, dz);
+    bool hit = r2 < pp.rc2;
+    double ir2 = rcp_nr(r2);
+    double u = ir2 * ir2 * ir2;
+    double W = fma(u, fma(48.0, u, -24.0), wq * r2);
+    double f = hit ? W * ir2 : 0.0;
+    double uh = hit ? u : 0.0;
+    a.su2 = fma(uh, uh, a.su2);
+    a.su += uh;
+    a.sr2 += hit ? r2 : 0.0;
+    a.nh += hit ? 1 : 0;
+    a.fx = fma(f, dx, a.fx);
+    a.fy = fma(f, dy, a.fy);
+    a.fz = fma(f, dz, a.fz);
+}
+
+// The atom's sum of pair energies and of pair virials (each pair counted in
+// both of its atoms' rows, halved by the finalize).
+__device__ __forceinline__ void lj_energy(const PairParams& pp, const LjSums& a, double& pe, double& w) {
+    const double bq = pp.beta * pp.inv_rc2, abq = pp.alpha - pp.beta, wq = -2.0 * pp.beta * pp.inv_rc2;
+    pe = fma(4.0, a.su2 - a.su, fma(bq, a.sr2, abq * (double)a.nh));
+    w = fma(48.0, a.su2, fma(-24.0, a.su, wq * a.sr2));
+}
+
 // Occupancy bound: 768 resident threads' worth of blocks per SM caps the kernel
 // at 80 registers (no spills); it is latency-bound on the neighbour gathers,
 // and 24 resident warps per SM measured ~12 % faster than 16 at 114 registers.
@@ -666,7 +703,8 @@ force_fp64_kernel(int N, const double4* __restrict__ pos, Soa s, const uint4* __
         const double4 xi = pos[i];
         bool near = !(xi.x >= pp.near_lo && xi.x < pp.near_hi[0] && xi.y >= pp.near_lo &&
                       xi.y < pp.near_hi[1] && xi.z >= pp.near_lo && xi.z < pp.near_hi[2]);
-        double fx = 0, fy = 0, fz = 0, pe = 0, w = 0;
+        LjSums a;        // KIND_LJ
+        double pe = 0, w = 0;  // KIND_CONST
         // list indices stream from HBM: two groups in flight ahead of the two
         // being evaluated
         int ng = (cnt[i] + 3) >> 2;
@@ -681,14 +719,19 @@ force_fp64_kernel(int N, const double4* __restrict__ pos, Soa s, const uint4* __
             for (int u = 0; u < 4; ++u) q[u] = ld_pos(pos + entry_slot(e[u]));
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                double dx, dy, dz, f, V, W;
+                double dx, dy, dz;
                 separation<SMALL>(xi, q[u], e[u], near, pp, dx, dy, dz);
-                pair_fp64<KIND>(pp, norm2(dx, dy, dz), f, V, W);
-                fx = fma(f, dx, fx);
-                fy = fma(f, dy, fy);
-                fz = fma(f, dz, fz);
-                pe += V;
-                w += W;
+                if (KIND == KIND_LJ) {
+                    lj_accumulate(pp, dx, dy, dz, a);
+                } else {
+                    double f, V, W;
+                    pair_fp64<KIND>(pp, norm2(dx, dy, dz), f, V, W);
+                    a.fx = fma(f, dx, a.fx);
+                    a.fy = fma(f, dy, a.fy);
+                    a.fz = fma(f, dz, a.fz);
+                    pe += V;
+                    w += W;
+                }
             }
         };
         for (int g = 0; g < ng; g += 2) {
@@ -699,13 +742,14 @@ force_fp64_kernel(int N, const double4* __restrict__ pos, Soa s, const uint4* __
             A = C;
             B = D;
         }
-        s.at(FX, i) = fx;
-        s.at(FY, i) = fy;
-        s.at(FZ, i) = fz;
+        if (KIND == KIND_LJ) lj_energy(pp, a, pe, w);
+        s.at(FX, i) = a.fx;
+        s.at(FY, i) = a.fy;
+        s.at(FZ, i) = a.fz;
         acc[1] = pe;
         acc[2] = w;
         if (KICK) {
-            const double f3[3] = {fx, fy, fz};
+            const double f3[3] = {a.fx, a.fy, a.fz};
             m = step_epilogue(N, i, s, xi, f3, pp, fu, acc);
         }
     }
