@@ -17,8 +17,10 @@
 // Pair forces are summed in FP32 over chunks of 8 consecutive neighbours and
 // each chunk sum is added into the FP64 per-atom accumulator, which keeps the
 // FP64 conversion traffic at one per chunk per component; PER_PAIR instead
-// converts and adds every pair's force, V and W in FP64 (no FP32 sum at all,
-// the mixed step 15 % slower at 1M atoms).  The loop structure
+// converts and adds every pair's terms in FP64 (no FP32 sum at all, the mixed
+// step 15 % slower at 1M atoms).  The energy and virial come, as on the FP64
+// path, from the power sums sum u^2, sum u, sum r^2 and the pair count
+// (lj_energy), formed in FP64 from the FP32 chunk sums.  The loop structure
 // (groups of 4 with the next group's indices in flight, branch-free cutoff) is
 // that of the FP64 kernel; the FP32 reciprocal is the hardware approximation
 // (rcp.approx, about 1 ulp), adequate for FP32 pair arithmetic.
@@ -31,9 +33,9 @@ namespace ljb {
 struct MixedParams {
     float rc2, inv_rc2, alpha, beta;
     float a[3];  // list-cell edge per axis
-    // the spline terms as functions of r^2: V = 4u(u - 1) + bq r^2 + abq,
-    // W = u(48u - 24) + wq r^2 with u = r^-6 (lennard_jones_force.cpp:107-119)
-    float bq, abq, wq;
+    // the spline's virial as a function of r^2: W = u(48u - 24) + wq r^2 with
+    // u = r^-6 (lennard_jones_force.cpp:107-119)
+    float wq;
 };
 
 inline MixedParams mixed_params(const PairParams& pp, const Grid& g) {
@@ -43,8 +45,6 @@ inline MixedParams mixed_params(const PairParams& pp, const Grid& g) {
     m.alpha = (float)pp.alpha;
     m.beta = (float)pp.beta;
     for (int k = 0; k < 3; ++k) m.a[k] = (float)(pp.L[k] / g.n[k]);
-    m.bq = (float)(pp.beta * pp.inv_rc2);
-    m.abq = (float)(pp.alpha - pp.beta);
     m.wq = (float)(-2.0 * pp.beta * pp.inv_rc2);
     return m;
 }
@@ -93,7 +93,7 @@ __device__ __forceinline__ float code_bias(unsigned e, unsigned field_mask) {
 }
 
 template <bool KICK, int BS = kThreads, bool PER_PAIR = false>
-static __global__ void __launch_bounds__(BS, 512 / BS)
+static __global__ void __launch_bounds__(BS, 768 / BS)
 force_mixed_kernel(int N, const float4* __restrict__ posl, Soa s, const uint4* __restrict__ nbr4,
                    const int* __restrict__ cnt, PairParams pp, MixedParams mp,
                    double* __restrict__ partials, Fuse fu) {
@@ -106,7 +106,10 @@ force_mixed_kernel(int N, const float4* __restrict__ posl, Soa s, const uint4* _
     if (i < N) {
         const float4 xi = posl[i];
         const float2 xi_xy = make_float2(xi.x, xi.y);
-        double fx = 0, fy = 0, fz = 0, pe = 0, w = 0;
+        // FP64 per-atom accumulators: the force and the power sums of the
+        // energy and virial (sum u^2, sum u, sum r^2, pair count; lj_energy)
+        double fx = 0, fy = 0, fz = 0, su2 = 0, su = 0, sr2 = 0;
+        int nh = 0;
         // list indices stream from HBM: two groups in flight ahead of the two
         // being evaluated (the neighbour positions, mostly L1/L2 hits, are
         // gathered per group)
@@ -117,7 +120,7 @@ force_mixed_kernel(int N, const float4* __restrict__ posl, Soa s, const uint4* _
         uint4 B = ng > 1 ? __ldcs(lp + (size_t)N) : z4;
         const float2 mone = make_float2(-1.f, -1.f);
         // one group: 4 neighbours into the FP32 chunk sums
-        auto group = [&](const uint4 grp, float& cx, float& cy, float& cz, float& cv, float& cw) {
+        auto group = [&](const uint4 grp, float& cx, float& cy, float& cz, float& cu2, float& cu, float& cr2) {
             float4 Q[4];
             gather4(posl, grp, Q);
             const unsigned e[4] = {grp.x, grp.y, grp.z, grp.w};
@@ -134,21 +137,25 @@ force_mixed_kernel(int N, const float4* __restrict__ posl, Soa s, const uint4* _
                 bool hit = r2 < mp.rc2;
                 float ir2 = rcp_approx(r2);
                 float ir6 = ir2 * ir2 * ir2;
-                float V = fmaf(4.f * ir6, ir6 - 1.f, fmaf(mp.bq, r2, mp.abq));
                 float W = fmaf(ir6, fmaf(48.f, ir6, -24.f), mp.wq * r2);
                 float f = hit ? W * ir2 : 0.f;
+                float uh = hit ? ir6 : 0.f;
+                float rh = hit ? r2 : 0.f;
+                nh += hit ? 1 : 0;
                 if (PER_PAIR) {
                     fx += (double)(f * dx);
                     fy += (double)(f * dy);
                     fz += (double)(f * dz);
-                    pe += (double)(hit ? V : 0.f);
-                    w += (double)(hit ? W : 0.f);
+                    su2 += (double)(uh * uh);
+                    su += (double)uh;
+                    sr2 += (double)rh;
                 } else {
                     cx = fmaf(f, dx, cx);
                     cy = fmaf(f, dy, cy);
                     cz = fmaf(f, dz, cz);
-                    cv += hit ? V : 0.f;
-                    cw += hit ? W : 0.f;
+                    cu2 = fmaf(uh, uh, cu2);
+                    cu += uh;
+                    cr2 += rh;
                 }
             }
         };
@@ -156,15 +163,16 @@ force_mixed_kernel(int N, const float4* __restrict__ posl, Soa s, const uint4* _
         for (int g = 0; g < ng; g += 2) {
             uint4 C = g + 2 < ng ? __ldcs(lp + (size_t)(g + 2) * N) : z4;
             uint4 D = g + 3 < ng ? __ldcs(lp + (size_t)(g + 3) * N) : z4;
-            float cx = 0.f, cy = 0.f, cz = 0.f, cv = 0.f, cw = 0.f;
-            group(A, cx, cy, cz, cv, cw);
-            if (g + 1 < ng) group(B, cx, cy, cz, cv, cw);
+            float cx = 0.f, cy = 0.f, cz = 0.f, cu2 = 0.f, cu = 0.f, cr2 = 0.f;
+            group(A, cx, cy, cz, cu2, cu, cr2);
+            if (g + 1 < ng) group(B, cx, cy, cz, cu2, cu, cr2);
             if (!PER_PAIR) {
                 fx += (double)cx;
                 fy += (double)cy;
                 fz += (double)cz;
-                pe += (double)cv;
-                w += (double)cw;
+                su2 += (double)cu2;
+                su += (double)cu;
+                sr2 += (double)cr2;
             }
             A = C;
             B = D;
@@ -172,8 +180,12 @@ force_mixed_kernel(int N, const float4* __restrict__ posl, Soa s, const uint4* _
         s.at(FX, i) = fx;
         s.at(FY, i) = fy;
         s.at(FZ, i) = fz;
-        acc[1] = pe;
-        acc[2] = w;
+        LjSums a;
+        a.su2 = su2;
+        a.su = su;
+        a.sr2 = sr2;
+        a.nh = nh;
+        lj_energy(pp, a, acc[1], acc[2]);
         if (KICK) {
             const double f3[3] = {fx, fy, fz};
             const double4 x = fu.pos_next ? fu.pos[i] : make_double4(0.0, 0.0, 0.0, 0.0);
