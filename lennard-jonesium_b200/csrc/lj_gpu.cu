@@ -106,6 +106,10 @@ struct lj_ctx {
     StepGraph graphs[2];
     bool graph_tried = false;
     int rebuild_kernels = 0;      // kernels in one rebuild chain
+    // the rebuild chain as a graph of its own, for the per-phase timing pass
+    cudaGraphExec_t rebuild_exec = nullptr;
+    bool rebuild_graph_tried = false;
+    int rebuild_graph_kernels = 0;
     char err[512] = {0};
 };
 
@@ -674,6 +678,32 @@ int enqueue_steps(lj_ctx* ctx, int nsteps) {
     return LJ_OK;
 }
 
+// The rebuild chain launched as one graph (the chain the step graphs run
+// behind their conditional node), so that in the per-phase pass its kernels
+// start back to back as inside a step graph instead of one host launch
+// apiece; direct launches if the capture is not available.
+int launch_rebuild_graph(lj_ctx* ctx) {
+    if (!ctx->rebuild_graph_tried) {
+        ctx->rebuild_graph_tried = true;
+        long long l0 = ctx->launches;
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            int rc = launch_rebuild(ctx);
+            cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+            if (rc != LJ_OK || e != cudaSuccess || cudaGraphInstantiate(&ctx->rebuild_exec, g, 0) != cudaSuccess)
+                ctx->rebuild_exec = nullptr;
+            if (g) cudaGraphDestroy(g);
+        }
+        ctx->rebuild_graph_kernels = (int)(ctx->launches - l0);
+        ctx->launches = l0;   // captured launches are not executions
+        cudaGetLastError();   // a failed capture leaves no error behind
+    }
+    if (!ctx->rebuild_exec) return launch_rebuild(ctx);
+    CK(cudaGraphLaunch(ctx->rebuild_exec, ctx->stream));
+    ctx->launches += ctx->rebuild_graph_kernels;
+    return LJ_OK;
+}
+
 int read_flags(lj_ctx* ctx) {
     Scalars h;
     CK(cudaMemcpyAsync(&h, ctx->sc, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
@@ -697,6 +727,7 @@ void free_all(lj_ctx* c) {
     if (c->host_ring) cudaFreeHost(c->host_ring);
     for (StepGraph& g : c->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (c->rebuild_exec) cudaGraphExecDestroy(c->rebuild_exec);
     if (c->side) cudaStreamDestroy(c->side);
     if (c->stream) cudaStreamDestroy(c->stream);
 }
@@ -1259,7 +1290,7 @@ int lj_gpu_step_timed(lj_ctx* ctx, int nsteps, lj_phase_times* out) {
             double d2;
             std::memcpy(&d2, &h.max_disp2, sizeof d2);
             bool open = gate.always || h.need_rebuild || d2 > gate.thresh2;
-            if (open && (rc = launch_rebuild(ctx))) return rc;
+            if (open && (rc = launch_rebuild_graph(ctx))) return rc;
         }
         CK(cudaEventRecord(ev[2], ctx->stream));
         if (forces) {
