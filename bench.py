@@ -300,7 +300,7 @@ def run_ours(args, ws, rank, local):
     for prec in ("fp64", "mixed"):
         extra = {"mixed_per_pair": True} if prec == "mixed" and args.mixed_per_pair else {}
         if args.autotune:
-            kw, tuned_ms = autotune(N_ATOMS, L, x, v, steps=100, cutoff=WORK["rc"], dt=WORK["dt"], precision=prec,
+            kw, tuned_ms = autotune(N_ATOMS, L, x, v, steps=256, cutoff=WORK["rc"], dt=WORK["dt"], precision=prec,
                                     device=local, **extra)
             tuning[prec] = dict(kw, tuned_ms_per_step=tuned_ms)
         else:

@@ -231,8 +231,9 @@ int lj_gpu_synchronize(lj_ctx* ctx);
 /* Device time of each phase of the step, accumulated over nsteps real steps
  * with CUDA events recorded between the phases on the context's stream.  The
  * host reads the rebuild criterion after each kick/drift (one synchronisation
- * per step) and launches the rebuild chain only when it holds, as one graph
- * launch (its kernels back to back, as inside the step graphs). */
+ * per step; that wait is part of no phase) and launches the rebuild chain
+ * only when it holds, as one graph launch (its kernels back to back, as
+ * inside the step graphs). */
 typedef struct lj_phase_times {
     double kick_drift_ms;  /* first half kick, drift, wrap, displacement check */
     double rebuild_ms;     /* cell binning + neighbour list, launched only on the steps whose

@@ -1269,7 +1269,9 @@ int lj_gpu_step_timed(lj_ctx* ctx, int nsteps, lj_phase_times* out) {
     if (!ctx || nsteps < 0 || !out) return set_err(ctx, LJ_ERR_ARG, "bad step arguments");
     CK(cudaSetDevice(ctx->p.device));
     std::memset(out, 0, sizeof *out);
-    cudaEvent_t ev[5];
+    // ev[1] after kick/drift, ev[5] once the host has read the rebuild
+    // criterion: the host round trip between them belongs to no phase
+    cudaEvent_t ev[6];
     for (auto& e : ev) CK(cudaEventCreate(&e));
     Scalars before;
     CK(cudaMemcpy(&before, ctx->sc, sizeof before, cudaMemcpyDeviceToHost));
@@ -1290,7 +1292,10 @@ int lj_gpu_step_timed(lj_ctx* ctx, int nsteps, lj_phase_times* out) {
             double d2;
             std::memcpy(&d2, &h.max_disp2, sizeof d2);
             bool open = gate.always || h.need_rebuild || d2 > gate.thresh2;
+            CK(cudaEventRecord(ev[5], ctx->stream));
             if (open && (rc = launch_rebuild_graph(ctx))) return rc;
+        } else {
+            CK(cudaEventRecord(ev[5], ctx->stream));
         }
         CK(cudaEventRecord(ev[2], ctx->stream));
         if (forces) {
@@ -1307,7 +1312,7 @@ int lj_gpu_step_timed(lj_ctx* ctx, int nsteps, lj_phase_times* out) {
         CK(cudaEventRecord(ev[4], ctx->stream));
         CK(cudaEventSynchronize(ev[4]));
         float ms[4];
-        for (int q = 0; q < 4; ++q) CK(cudaEventElapsedTime(&ms[q], ev[q], ev[q + 1]));
+        for (int q = 0; q < 4; ++q) CK(cudaEventElapsedTime(&ms[q], ev[q == 1 ? 5 : q], ev[q + 1]));
         out->kick_drift_ms += ms[0];
         out->rebuild_ms += ms[1];
         out->force_ms += ms[2];
