@@ -43,7 +43,7 @@ extern "C" {
 #define LJ_ERR_ARG 1        /* invalid argument (bad size, box below cutoff, null pointer) */
 #define LJ_ERR_CUDA 2       /* a CUDA call failed; lj_gpu_last_error() has the message */
 #define LJ_ERR_NONFINITE 3  /* a non-finite energy or virial appeared during a step */
-#define LJ_ERR_TIMEOUT 4    /* a bounded device-side wait gave up */
+#define LJ_ERR_TIMEOUT 4    /* a bounded device-side loop reached its bound (lj_batch_step) */
 #define LJ_ERR_CAPACITY 5   /* a neighbour list overflowed its capacity; results are invalid */
 
 /* Arithmetic of the pair kernel. */

@@ -116,7 +116,7 @@ struct lj_ctx {
 namespace {
 
 const char* kStatus[] = {"ok", "invalid argument", "CUDA error", "non-finite energy or virial",
-                         "device wait timed out", "neighbour list capacity exceeded"};
+                         "device loop reached its bound", "neighbour list capacity exceeded"};
 
 int set_err(lj_ctx* c, int code, const char* msg) {
     if (c) std::snprintf(c->err, sizeof c->err, "%s", msg);
