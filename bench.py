@@ -469,6 +469,7 @@ def run_sweep_bench(args):
     b = ctypes.c_void_p()
     nat.check(lib.lj_batch_create(table, nsys, SWEEP["rc"], 0, ctypes.byref(b)))
     nat.check(lib.lj_batch_set_force_block(b, tune.force_block))
+    nat.check(lib.lj_batch_set_list_tile(b, tune.list_cells_per_block))
     for s, sy in enumerate(systems):
         nat.check(lib.lj_batch_upload_system(b, s, P(sy["x"]), P(sy["v"]), 4))
     recs = np.zeros((chunk, nsys, 7))
@@ -508,6 +509,7 @@ def run_sweep_bench(args):
             "systems": nsys, "atoms": atoms, "steps": total_steps,
             "identical_final_records": bool(np.array_equal(final_batched, final_seq)),
             "tuning": {"skin": tune.skin, "force_block": tune.force_block,
+                       "list_cells_per_block": tune.list_cells_per_block,
                        "tuned_ms_per_step": tune.ms_per_step, "source": "lj_batch_autotune, 200 steps per candidate"},
             "run_sweep_files": files,
             "config": {"workload": "8x8 grid rho in [0.05,1.0] x T in [0.5,2.0], N=4n^3, n~U{5..20} (seed 2024), "

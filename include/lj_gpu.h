@@ -395,16 +395,21 @@ int lj_batch_step(lj_batch* batch, int nsteps, lj_thermo* out);
  * evolves bit for bit as it does alone. */
 int lj_batch_set_force_block(lj_batch* batch, int force_block);
 
+/* List cells per block of the batch's list build (one warp per cell): 2, 4
+ * (the default) or 8.  The lists do not depend on it. */
+int lj_batch_set_list_tile(lj_batch* batch, int cells);
+
 /* Batch autotuner (the batched counterpart of lj_gpu_autotune): times `steps`
  * steps of the whole batch for every candidate Verlet skin (0.2, 0.3, 0.4, 0.5,
- * each clipped by the box as in lj_gpu_create) and pair-kernel block size (64,
- * 128, 256), each in a fresh batch from the state x, v (every system's atoms
- * in table order, stride doubles per atom; v may be NULL), and writes the
- * fastest to *best.  The per-step work depends only on these two knobs: the
- * list build's tiling (a warp per cell) and one atom per thread are fixed. */
+ * each clipped by the box as in lj_gpu_create), pair-kernel block size (64,
+ * 128, 256) and list-build tile (2, 4, 8 cells per block), each in a fresh
+ * batch from the state x, v (every system's atoms in table order, stride
+ * doubles per atom; v may be NULL), and writes the fastest to *best.  The
+ * pair kernel runs one atom per thread in every candidate. */
 typedef struct lj_batch_tuning {
     double skin;
     int force_block;
+    int list_cells_per_block;
     double ms_per_step;
 } lj_batch_tuning;
 int lj_batch_autotune(const lj_batch_system* systems, int nsys, double cutoff, int device, const double* x,

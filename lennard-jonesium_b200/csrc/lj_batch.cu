@@ -261,16 +261,18 @@ b_copy_back_kernel(const int* __restrict__ sys_of, const SysState* st, int Ntot,
 
 // Warp-per-cell list build: the per-cell body of build_list_warp_kernel, on
 // the grid and slot ranges of the cell's own system (entries identical to a
-// single-system build of that system).  Six resident blocks leave it up to 80
-// registers, where it does not spill (the per-system indexing costs the
-// registers the single-system kernel fits into 64).
-static __global__ void __launch_bounds__(32 * kBuildWarps, 6)
+// single-system build of that system).  W cells (warps) per block, the list
+// tile a batch tunes; 24 resident warps leave it up to 80 registers, where it
+// does not spill (the per-system indexing costs the registers the
+// single-system kernel fits into 64).
+template <int W>
+static __global__ void __launch_bounds__(32 * W, 24 / W)
 b_build_list_kernel(const int* __restrict__ cell_sys, const SysDev* __restrict__ sys, SysState* st, int ncell_tot,
                     int Ntot, const float4* __restrict__ posf, const int* __restrict__ start, int cap,
                     uint4* __restrict__ nbr4, int* __restrict__ cnt, BatchFlags* fl) {
-    __shared__ BuildSmem bs[kBuildWarps];
+    __shared__ BuildSmem bs[W];
     int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int c = blockIdx.x * kBuildWarps + warp;
+    int c = blockIdx.x * W + warp;
     if (c >= ncell_tot) return;
     int sidx = cell_sys[c];
     if (!sys_rebuild(st, sidx)) return;
@@ -458,6 +460,7 @@ struct lj_batch {
     BatchFlags* fl = nullptr;
     int *blk_sys = nullptr, *blk_first = nullptr, *sys_of = nullptr, *cell_sys = nullptr;
     int force_block = kThreads, nfblk = 0;
+    int list_tile = kBuildWarps;  // list cells (warps) per block of the list build
     int *fblk_sys = nullptr, *fblk_first = nullptr;  // pair-kernel block tables (room for 64-atom blocks)
     double4 *pos = nullptr, *pos_tmp = nullptr;
     float4* posf = nullptr;
@@ -520,8 +523,14 @@ int launch_rebuild_b(lj_batch* b) {
     b_copy_back_kernel<<<nb(b->Ntot), kThreads, 0, b->stream>>>(b->sys_of, b->st, b->Ntot, b->pos_tmp, b->pos, st, s,
                                                                 b->ids_tmp, b->ids, b->posf);
     BKL();
-    b_build_list_kernel<<<nb(b->ncell, kBuildWarps), 32 * kBuildWarps, 0, b->stream>>>(
-        b->cell_sys, b->sys, b->st, b->ncell, b->Ntot, b->posf, b->start, b->cap, b->nbr, b->cnt, b->fl);
+#define LJ_BBUILD(W)                                                                                 \
+    b_build_list_kernel<W><<<nb(b->ncell, W), 32 * W, 0, b->stream>>>(b->cell_sys, b->sys, b->st, b->ncell, \
+                                                                      b->Ntot, b->posf, b->start, b->cap,   \
+                                                                      b->nbr, b->cnt, b->fl)
+    if (b->list_tile == 2) LJ_BBUILD(2);
+    else if (b->list_tile == 8) LJ_BBUILD(8);
+    else LJ_BBUILD(4);
+#undef LJ_BBUILD
     BKL();
     return LJ_OK;
 }
@@ -1052,6 +1061,18 @@ int lj_batch_set_force_block(lj_batch* b, int force_block) {
     return set_force_blocks(b, force_block);
 }
 
+int lj_batch_set_list_tile(lj_batch* b, int cells) {
+    if (!b || (cells != 2 && cells != 4 && cells != 8)) return LJ_ERR_ARG;
+    BK(cudaSetDevice(b->device));
+    BK(cudaStreamSynchronize(b->stream));
+    b->list_tile = cells;
+    if (b->graph) cudaGraphExecDestroy(b->graph);  // the chunk graph holds the old launch shape
+    b->graph = nullptr;
+    b->graph_steps = 0;
+    b->graph_tried = false;
+    return LJ_OK;
+}
+
 int lj_batch_set_iteration_limit(lj_batch* b, int limit) {
     if (!b || limit < 0) return LJ_ERR_ARG;
     b->loop_limit_override = limit;
@@ -1074,23 +1095,26 @@ int lj_batch_window_stats(lj_batch* b, int sample_size, const double* density, l
 }
 
 // Batch autotuner: every candidate (Verlet skin of all systems x pair-kernel
-// block size) runs in a fresh batch from the caller's state -- 16 steps to
-// build the chunk graph and the first lists, then `steps` timed steps -- and
-// the fastest is returned.
+// block size x list cells per list-build block) runs in a fresh batch from the
+// caller's state -- 16 steps to build the chunk graph and the first lists,
+// then `steps` timed steps -- and the fastest is returned.
 int lj_batch_autotune(const lj_batch_system* systems, int nsys, double cutoff, int device, const double* x,
                       const double* v, int stride, int steps, lj_batch_tuning* best) {
     if (!systems || nsys < 1 || !x || !best || steps < 8 || (stride != 3 && stride != 4)) return LJ_ERR_ARG;
     const double skins[] = {0.2, 0.3, 0.4, 0.5};
     const int blocks[] = {64, 128, 256};
+    const int tiles[] = {2, 4, 8};
     std::vector<lj_batch_system> table(systems, systems + nsys);
-    lj_batch_tuning win{-1.0, 0, 1e300};
+    lj_batch_tuning win{-1.0, 0, 0, 1e300};
     for (double sk : skins) {
         for (lj_batch_system& q : table) q.skin = sk;
-        for (int bs : blocks) {
+        for (int cand = 0; cand < 9; ++cand) {
+            int bs = blocks[cand / 3], tile = tiles[cand % 3];
             lj_batch* b = nullptr;
             int rc = lj_batch_create(table.data(), nsys, cutoff, device, &b);
             if (rc) return rc;
             rc = lj_batch_set_force_block(b, bs);
+            if (!rc) rc = lj_batch_set_list_tile(b, tile);
             size_t off = 0;
             for (int s = 0; s < nsys && !rc; ++s) {
                 rc = lj_batch_upload_system(b, s, x + off, v ? v + off : nullptr, stride);
@@ -1111,7 +1135,7 @@ int lj_batch_autotune(const lj_batch_system* systems, int nsys, double cutoff, i
             if (e1) cudaEventDestroy(e1);
             lj_batch_destroy(b);
             if (rc) return rc;
-            if (ms / steps < win.ms_per_step) win = lj_batch_tuning{sk, bs, (double)ms / steps};
+            if (ms / steps < win.ms_per_step) win = lj_batch_tuning{sk, bs, tile, (double)ms / steps};
         }
     }
     *best = win;

@@ -100,7 +100,8 @@ class Observation(ctypes.Structure):
 
 
 class BatchTuning(ctypes.Structure):
-    _fields_ = [("skin", ctypes.c_double), ("force_block", ctypes.c_int), ("ms_per_step", ctypes.c_double)]
+    _fields_ = [("skin", ctypes.c_double), ("force_block", ctypes.c_int), ("list_cells_per_block", ctypes.c_int),
+                ("ms_per_step", ctypes.c_double)]
 
 
 class LJError(RuntimeError):
@@ -161,6 +162,7 @@ SIGNATURES = {
     "lj_batch_step": (ctypes.c_int, [P, ctypes.c_int, P]),
     "lj_batch_set_iteration_limit": (ctypes.c_int, [P, ctypes.c_int]),
     "lj_batch_set_force_block": (ctypes.c_int, [P, ctypes.c_int]),
+    "lj_batch_set_list_tile": (ctypes.c_int, [P, ctypes.c_int]),
     "lj_batch_autotune": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double, ctypes.c_int, P, P, ctypes.c_int,
                                          ctypes.c_int, P]),
     "lj_batch_measure": (ctypes.c_int, [P, P]),

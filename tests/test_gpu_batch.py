@@ -38,7 +38,7 @@ def _table(states, L, skin=-1.0):
     return systems
 
 
-def _batch(states, L, skin=-1.0, force_block=0):
+def _batch(states, L, skin=-1.0, force_block=0, list_tile=0):
     from lennardjonesium import _native as nat
     lib = nat.lib()
     n = len(states)
@@ -47,6 +47,8 @@ def _batch(states, L, skin=-1.0, force_block=0):
     nat.check(lib.lj_batch_create(systems, n, 2.5, 0, ctypes.byref(b)))
     if force_block:
         nat.check(lib.lj_batch_set_force_block(b, force_block))
+    if list_tile:
+        nat.check(lib.lj_batch_set_list_tile(b, list_tile))
     for s, (x, v) in enumerate(states):
         nat.check(lib.lj_batch_upload_system(b, s, x.ctypes.data_as(ctypes.c_void_p),
                                              v.ctypes.data_as(ctypes.c_void_p), 4))
@@ -217,17 +219,18 @@ def test_batch_chunk_loop_bound():
     assert np.array_equal(recs[:, 0, :], ref)
 
 
-@pytest.mark.parametrize("skin,block", [(0.4, 64), (0.2, 256)])
-def test_tuned_batch_equals_single_systems(skin, block):
-    """A batch run with another skin and pair-kernel block size (autotuner
-    candidates) equals single-system runs with the same parameters bit for bit."""
+@pytest.mark.parametrize("skin,block,tile", [(0.4, 64, 2), (0.2, 256, 8)])
+def test_tuned_batch_equals_single_systems(skin, block, tile):
+    """A batch run with another skin, pair-kernel block size and list-build tile
+    (autotuner candidates) equals single-system runs with the same skin and
+    block size bit for bit."""
     from lennardjonesium import GpuSystem
     states, L = [], []
     for N, T, rho, seed in SYSTEMS[:4]:
         x, v, box = ljref.initial_state(N, T, rho, seed)
         states.append((x, v))
         L.append(box)
-    lib, b = _batch(states, L, skin=skin, force_block=block)
+    lib, b = _batch(states, L, skin=skin, force_block=block, list_tile=tile)
     recs = np.zeros((90, len(states), 7))
     try:
         assert lib.lj_batch_step(b, 90, recs.ctypes.data_as(ctypes.c_void_p)) == 0
@@ -254,3 +257,4 @@ def test_batch_autotune_returns_a_candidate():
                                      v.ctypes.data_as(ctypes.c_void_p), 4, 16, ctypes.byref(best))
     assert rc == 0
     assert best.skin in (0.2, 0.3, 0.4, 0.5) and best.force_block in (64, 128, 256) and best.ms_per_step > 0
+    assert best.list_cells_per_block in (2, 4, 8)
