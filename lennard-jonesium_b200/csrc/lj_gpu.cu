@@ -103,8 +103,6 @@ struct lj_ctx {
     // step graphs: kick_drift -> decide -> IF(rebuild chain) -> force -> finalize, unrolled;
     // a long one for runs of steps and a short one for the remainder
     cudaStream_t side = nullptr;  // captures the conditional body
-    cudaStream_t aux = nullptr;   // the copy back, beside the list build
-    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     StepGraph graphs[2];
     bool graph_tried = false;
     int rebuild_kernels = 0;      // kernels in one rebuild chain
@@ -220,28 +218,12 @@ int launch_rebuild(lj_ctx* ctx) {
     CKL();
     gather_kernel<<<blocks_for(N), kThreads, 0, ctx->stream>>>(
         N, ctx->order, ctx->pos, ctx->pos_tmp, soa_of(ctx->soa, N), soa_of(ctx->soa_tmp, N), ctx->ids,
-        ctx->ids_tmp, ctx->bd, ctx->posf, gate);
+        ctx->ids_tmp, ctx->bd, gate);
     CKL();
-    // the warp list build reads only the FP32 copy and the cell ranges: the
-    // copy back of the permuted state (and the mixed path's cell-local
-    // coordinates, which read it) run beside it on the second stream, which
-    // joins again before the pair kernel; small boxes keep one stream (their
-    // build reads the FP64 positions)
-    const bool fork = !ctx->small_box;
-    cudaStream_t cb = ctx->stream;
-    if (fork) {
-        CK(cudaEventRecord(ctx->fork_ev, ctx->stream));
-        CK(cudaStreamWaitEvent(ctx->aux, ctx->fork_ev, 0));
-        cb = ctx->aux;
-    }
-    copy_back_kernel<<<blocks_for(N), kThreads, 0, cb>>>(
-        N, ctx->pos_tmp, ctx->pos, soa_of(ctx->soa_tmp, N), soa_of(ctx->soa, N), ctx->ids_tmp, ctx->ids, gate);
+    copy_back_kernel<<<blocks_for(N), kThreads, 0, ctx->stream>>>(
+        N, ctx->pos_tmp, ctx->pos, soa_of(ctx->soa_tmp, N), soa_of(ctx->soa, N), ctx->ids_tmp, ctx->ids,
+        ctx->posf, gate);
     CKL();
-    if (ctx->p.precision == LJ_PRECISION_MIXED) {
-        mixed_build_local_kernel<<<blocks_for(N), kThreads, 0, cb>>>(
-            N, ctx->pos, soa_of(ctx->soa, N), ctx->list_grid, ctx->bx, ctx->posl, gate);
-        CKL();
-    }
     // FP32 candidate radius, widened past FP32 rounding of box coordinates so the
     // list is a superset of the FP64 pair set
     double Lmax = std::max(ctx->pp.L[0], std::max(ctx->pp.L[1], ctx->pp.L[2]));
@@ -255,9 +237,10 @@ int launch_rebuild(lj_ctx* ctx) {
         build_list_warp_kernel<<<blocks_for(ctx->list_grid.ncell(), kBuildWarps), 32 * kBuildWarps, 0, ctx->stream>>>(
             N, ctx->pos, ctx->posf, ctx->list_grid, ctx->start, Lf, cut2, ctx->cap, ctx->nbr, ctx->cnt, ctx->sc, gate);
     CKL();
-    if (fork) {
-        CK(cudaEventRecord(ctx->join_ev, ctx->aux));
-        CK(cudaStreamWaitEvent(ctx->stream, ctx->join_ev, 0));
+    if (ctx->p.precision == LJ_PRECISION_MIXED) {
+        mixed_build_local_kernel<<<blocks_for(N), kThreads, 0, ctx->stream>>>(
+            N, ctx->pos, soa_of(ctx->soa, N), ctx->list_grid, ctx->bx, ctx->posl, gate);
+        CKL();
     }
     return LJ_OK;
 }
@@ -746,9 +729,6 @@ void free_all(lj_ctx* c) {
         if (g.exec) cudaGraphExecDestroy(g.exec);
     if (c->rebuild_exec) cudaGraphExecDestroy(c->rebuild_exec);
     if (c->side) cudaStreamDestroy(c->side);
-    if (c->aux) cudaStreamDestroy(c->aux);
-    if (c->fork_ev) cudaEventDestroy(c->fork_ev);
-    if (c->join_ev) cudaEventDestroy(c->join_ev);
     if (c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -760,9 +740,6 @@ int init_ctx(lj_ctx* ctx, const lj_params& p) {
     CK(cudaSetDevice(p.device));
     CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
-    CK(cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking));
-    CK(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
-    CK(cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming));
 
     // pair constants (lennard_jones_force.cpp:33-74)
     PairParams& pp = ctx->pp;

@@ -217,20 +217,16 @@ cell_sort_kernel(int ncell, const int* __restrict__ start, int* __restrict__ ord
         }
 }
 
-// Gather the state into sorted order (into the scratch copies), with the FP32
-// position copy the list build reads, so that the build need not wait for the
-// copy back.
+// Gather the state into sorted order (into the scratch copies).
 static __global__ void __launch_bounds__(kThreads)
 gather_kernel(int N, const int* __restrict__ order, const double4* __restrict__ pos,
               double4* __restrict__ pos_out, Soa s, Soa s_out, const int* __restrict__ ids,
-              int* __restrict__ ids_out, double* __restrict__ bd, float4* __restrict__ posf, Gate gate) {
+              int* __restrict__ ids_out, double* __restrict__ bd, Gate gate) {
     if (!gate.open()) return;
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= N) return;
     int o = order[k];
-    double4 x = pos[o];
-    pos_out[k] = x;
-    posf[k] = make_float4((float)x.x, (float)x.y, (float)x.z, 0.f);
+    pos_out[k] = pos[o];
 #pragma unroll
     for (int f = 0; f < SOA_FIELDS; ++f) s_out.at(f, k) = s.at(f, o);
     ids_out[k] = ids[o];
@@ -238,15 +234,17 @@ gather_kernel(int N, const int* __restrict__ order, const double4* __restrict__ 
     for (int q = 0; q < 3; ++q) bd[(size_t)q * N + k] = s.at(DX + q, o);
 }
 
-// Copy the sorted state back (it runs beside the list build, which reads only
-// the FP32 copy the gather wrote).
+// Copy the sorted state back and write the FP32 position copy used by the list build.
 static __global__ void __launch_bounds__(kThreads)
 copy_back_kernel(int N, const double4* __restrict__ pos_in, double4* __restrict__ pos, Soa s_in,
-                 Soa s, const int* __restrict__ ids_in, int* __restrict__ ids, Gate gate) {
+                 Soa s, const int* __restrict__ ids_in, int* __restrict__ ids, float4* __restrict__ posf,
+                 Gate gate) {
     if (!gate.open()) return;
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= N) return;
-    pos[k] = pos_in[k];
+    double4 x = pos_in[k];
+    pos[k] = x;
+    posf[k] = make_float4((float)x.x, (float)x.y, (float)x.z, 0.f);
 #pragma unroll
     for (int f = 0; f < SOA_FIELDS; ++f) s.at(f, k) = s_in.at(f, k);
     ids[k] = ids_in[k];
