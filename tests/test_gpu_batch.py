@@ -258,3 +258,44 @@ def test_batch_autotune_returns_a_candidate():
     assert rc == 0
     assert best.skin in (0.2, 0.3, 0.4, 0.5) and best.force_block in (64, 128, 256) and best.ms_per_step > 0
     assert best.list_cells_per_block in (2, 4, 8)
+
+
+def test_batch_anisotropic_system_equals_single():
+    """A batch holding an anisotropic box beside a cubic one: each system evolves
+    bit for bit as it does alone."""
+    from lennardjonesium import GpuSystem
+    from lennardjonesium import _native as nat
+    rng = np.random.default_rng(21)
+    n = (8, 10, 13)
+    a = 1.0772
+    g = np.stack(np.meshgrid(*[np.arange(k) for k in n], indexing="ij"), axis=-1).reshape(-1, 3)
+    La = np.array(n, dtype=float) * a
+    xa = np.zeros((g.shape[0], 4))
+    xa[:, :3] = np.mod((g + 0.5) * a + rng.uniform(-0.1, 0.1, size=g.shape), La)
+    va = np.zeros_like(xa)
+    va[:, :3] = rng.normal(0.0, 1.0, size=(g.shape[0], 3))
+    va[:, :3] -= va[:, :3].mean(axis=0)
+    xc, vc, Lc = ljref.initial_state(864, 0.722, 0.8442, 5489)
+    systems = (nat.BatchSystem * 2)()
+    for s, (x, box) in enumerate(((xa, La), (xc, np.full(3, Lc)))):
+        systems[s].particle_count = x.shape[0]
+        for k in range(3):
+            systems[s].box[k] = box[k]
+        systems[s].time_delta = 0.005
+        systems[s].skin = -1.0
+    lib = nat.lib()
+    b = ctypes.c_void_p()
+    nat.check(lib.lj_batch_create(systems, 2, 2.5, 0, ctypes.byref(b)))
+    P = lambda q: q.ctypes.data_as(ctypes.c_void_p)
+    recs = np.zeros((120, 2, 7))
+    try:
+        for s, (x, v) in enumerate(((xa, va), (xc, vc))):
+            nat.check(lib.lj_batch_upload_system(b, s, P(x), P(v), 4))
+        assert lib.lj_batch_step(b, 120, P(recs)) == 0
+    finally:
+        lib.lj_batch_destroy(b)
+    for s, (x, v, box) in enumerate(((xa, va, La), (xc, vc, Lc))):
+        with GpuSystem(x.shape[0], box) as gs:
+            gs.upload(x, v=v)
+            ref = gs.step(120)
+        assert np.array_equal(recs[:, s, :], ref), f"system {s}"

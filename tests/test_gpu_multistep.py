@@ -23,8 +23,10 @@ arithmetic, so multi-step runs are judged on what survives the divergence:
     time whenever a change of rounding reshuffles the trajectories;
   * the 4 000 000-atom system (4 * 100^3, rho 0.8, T 0.9, dt 0.004): single-step
     forces within 1e-12 of each atom's sum of |pair forces|, PE and virial
-    within 1e-12 relative of the oracle, and the RDF (200 bins to 4 sigma)
-    bit-exact against the oracle's histogram.
+    within 1e-12 relative of the oracle, the RDF (200 bins to 4 sigma)
+    bit-exact against the oracle's histogram, and the mixed path's forces
+    within its stated bounds (1e-5 of the sum of |pair forces|, PE 1e-6 and
+    virial 1e-5 relative).
 """
 
 import concurrent.futures as cf
@@ -141,3 +143,11 @@ def test_four_million_atoms_forces_and_rdf():
     assert st["pe"] == pytest.approx(pe, rel=1e-12)
     assert st["virial"] == pytest.approx(w, rel=1e-12)
     assert np.array_equal(h, ljref.rdf_cells(xs, L, 200, 4.0))
+    # config 5 runs the mixed path: its forces at the same positions, within the stated bounds
+    with gpu_system(N, L, dt=0.004, precision="mixed") as g:
+        g.upload(xs)
+        pe32, w32 = g.compute_forces()
+        F32 = g.download()["F"]
+    e32 = np.sqrt(np.sum((F32 - Fref)[:, :3] ** 2, axis=1))
+    assert np.all(e32 <= 1e-5 * S)
+    assert abs(pe32 - pe) / abs(pe) < 1e-6 and abs(w32 - w) / abs(w) < 1e-5

@@ -469,3 +469,38 @@ def test_mixed_full_size_force_error(per_pair):
     assert np.sqrt(np.mean(err ** 2)) / rms < 2e-5
     assert abs(pe32 - pe64) / abs(pe64) < 1e-6
     assert abs(w32 - w64) / abs(w64) < 1e-5
+
+
+def _anisotropic_lattice(n=(12, 16, 24), a=1.0772, amp=0.1, seed=12):
+    """A perturbed simple-cubic lattice in an anisotropic box (rho ~ 0.8)."""
+    g = np.stack(np.meshgrid(*[np.arange(k) for k in n], indexing="ij"), axis=-1).reshape(-1, 3)
+    L = np.array(n, dtype=float) * a
+    rng = np.random.default_rng(seed)
+    x = np.mod((g + 0.5) * a + rng.uniform(-amp, amp, size=g.shape), L)
+    return x, L
+
+
+def test_anisotropic_box_both_paths_and_rdf():
+    """An anisotropic box of 4608 atoms (12 x 16 x 24 cells of the lattice): the
+    FP64 pair set bit-exact and forces at 1e-12, the mixed path within its
+    bounds, the RDF bit-exact, all against the oracle."""
+    x, L = _anisotropic_lattice()
+    N = x.shape[0]
+    with gpu_system(N, L) as g:
+        g.upload(x)
+        assert pair_key(*g.debug_pairs()) == oracle_pair_key(x, L, 2.5)
+        pe64, w64 = g.compute_forces()
+        F64 = g.download()["F"]
+        h = g.rdf(160, 4.0)
+    Fref, pe, w = ljref.forces(x, L, 2.5)
+    S = ljref.force_abs_sum(x, L, 2.5)
+    assert_forces(F64, Fref, S)
+    assert pe64 == pytest.approx(pe, rel=1e-12) and w64 == pytest.approx(w, rel=1e-12)
+    assert np.array_equal(h, ljref.rdf(x, L, 160, 4.0))
+    with gpu_system(N, L, precision="mixed") as g:
+        g.upload(x)
+        pe32, w32 = g.compute_forces()
+        F32 = g.download()["F"]
+    err = np.sqrt(np.sum((F32 - F64)[:, :3] ** 2, axis=1))
+    assert np.all(err <= 1e-5 * S)
+    assert abs(pe32 - pe64) / abs(pe64) < 1e-6 and abs(w32 - w64) / abs(w64) < 1e-5
