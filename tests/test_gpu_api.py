@@ -143,3 +143,29 @@ def test_trajectory_frames_equal_downloads(tmp_path, precision):
         g.synchronize()
         assert g.trajectory_close() == 3
     assert path.read_text() == "\n".join(want) + "\n"
+
+
+def test_equilibration_reaches_a_new_temperature():
+    """tests/cpp/integration/test_system_equilibration.cpp, loose phase: N = 100 at
+    rho 0.8, rc 2.0 (two list cells per axis), started at T 0.3 and driven to 0.8
+    by the equilibration rule (every 100 steps, rescale to the target when the
+    mean T of the last 50 steps is off by >= 10 %; done after 5000 steps without
+    a rescale).  The temperature then measured as the mean of 20 samples 5
+    steps apart is within 10 % of 0.8."""
+    from lennardjonesium import GpuSystem
+    x, v, L = ljref.initial_state(100, 0.3, 0.8, 5489)
+    with GpuSystem(100, L, cutoff=2.0) as g:
+        g.upload(x, v=v)
+        steady = 0
+        for _ in range(500):  # the reference's timeout: 50 000 steps
+            recs = g.step(100)
+            if abs(recs[-50:, 5].mean() / 0.8 - 1.0) >= 0.10:
+                g.set_temperature(0.8)
+                steady = 0
+            else:
+                steady += 100
+                if steady >= 5000:
+                    break
+        assert steady >= 5000
+        T = np.mean([g.step(5)[-1, 5] for _ in range(20)])
+    assert abs(T / 0.8 - 1.0) < 0.10

@@ -504,3 +504,15 @@ def test_anisotropic_box_both_paths_and_rdf():
     err = np.sqrt(np.sum((F32 - F64)[:, :3] ** 2, axis=1))
     assert np.all(err <= 1e-5 * S)
     assert abs(pe32 - pe64) / abs(pe64) < 1e-6 and abs(w32 - w64) / abs(w64) < 1e-5
+
+
+def test_measurement_rotating_cube():
+    """physics/test_measurements.cpp: four atoms on a cube rotating about z,
+    KE = 4 and T = (8/3) / 4, measured on the GPU (no force calculation)."""
+    x = np.array([[0, 0, 0], [0, 0, 2], [2, 2, 0], [2, 2, 2]], dtype=float)
+    v = np.array([[1, -1, 0], [1, -1, 0], [-1, 1, 0], [-1, 1, 0]], dtype=float)
+    with gpu_system(4, 10.0, force="none", periodic=False) as g:
+        g.upload(x, v=v)
+        m = g.measure()
+    assert m[1] == 4.0 and m[5] == pytest.approx(8 / 3 / 4, rel=1e-15)
+    assert m[2] == 0.0 and m[4] == 0.0 and m[6] == 0.0
