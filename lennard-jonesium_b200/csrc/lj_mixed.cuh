@@ -119,8 +119,9 @@ force_mixed_kernel(int N, const float4* __restrict__ posl, Soa s, const uint4* _
         uint4 A = ng > 0 ? __ldcs(lp) : z4;
         uint4 B = ng > 1 ? __ldcs(lp + (size_t)N) : z4;
         const float2 mone = make_float2(-1.f, -1.f);
-        // one group: 4 neighbours into the FP32 chunk sums
-        auto group = [&](const uint4 grp, float& cx, float& cy, float& cz, float& cu2, float& cu, float& cr2) {
+        // one group: 4 neighbours into the FP32 chunk sums, (x, y) of the force
+        // and (sum u^2, sum u) as packed pairs
+        auto group = [&](const uint4 grp, float2& cxy, float& cz, float2& cuu, float& cr2) {
             float4 Q[4];
             gather4(posl, grp, Q);
             const unsigned e[4] = {grp.x, grp.y, grp.z, grp.w};
@@ -150,11 +151,9 @@ force_mixed_kernel(int N, const float4* __restrict__ posl, Soa s, const uint4* _
                     su += (double)uh;
                     sr2 += (double)rh;
                 } else {
-                    cx = fmaf(f, dx, cx);
-                    cy = fmaf(f, dy, cy);
+                    cxy = __ffma2_rn(make_float2(f, f), d_xy, cxy);
                     cz = fmaf(f, dz, cz);
-                    cu2 = fmaf(uh, uh, cu2);
-                    cu += uh;
+                    cuu = __ffma2_rn(make_float2(uh, uh), make_float2(uh, 1.f), cuu);
                     cr2 += rh;
                 }
             }
@@ -163,15 +162,16 @@ force_mixed_kernel(int N, const float4* __restrict__ posl, Soa s, const uint4* _
         for (int g = 0; g < ng; g += 2) {
             uint4 C = g + 2 < ng ? __ldcs(lp + (size_t)(g + 2) * N) : z4;
             uint4 D = g + 3 < ng ? __ldcs(lp + (size_t)(g + 3) * N) : z4;
-            float cx = 0.f, cy = 0.f, cz = 0.f, cu2 = 0.f, cu = 0.f, cr2 = 0.f;
-            group(A, cx, cy, cz, cu2, cu, cr2);
-            if (g + 1 < ng) group(B, cx, cy, cz, cu2, cu, cr2);
+            float2 cxy = make_float2(0.f, 0.f), cuu = make_float2(0.f, 0.f);
+            float cz = 0.f, cr2 = 0.f;
+            group(A, cxy, cz, cuu, cr2);
+            if (g + 1 < ng) group(B, cxy, cz, cuu, cr2);
             if (!PER_PAIR) {
-                fx += (double)cx;
-                fy += (double)cy;
+                fx += (double)cxy.x;
+                fy += (double)cxy.y;
                 fz += (double)cz;
-                su2 += (double)cu2;
-                su += (double)cu;
+                su2 += (double)cuu.x;
+                su += (double)cuu.y;
                 sr2 += (double)cr2;
             }
             A = C;
