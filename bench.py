@@ -436,6 +436,34 @@ def sweep_files_arm():
                       "2000, timeout 10000; obs: 10 x 500 steps; four files per run"}
 
 
+def batch_window_stats(lib, b, systems, recs, reps=50):
+    """ThermodynamicAnalyzer over each system's last len(recs) records: all systems
+    in one device call (lj_batch_window_stats, from the batch's record ring)
+    against the host restatement over the same records, which the host must
+    first hold (recs: the last chunk's records, steps x systems x 7)."""
+    import numpy as np
+    from lennardjonesium import _native as nat
+    from lennardjonesium import window_stats_host
+    W, nsys = recs.shape[0], recs.shape[1]
+    dens = np.array([sy["N"] / sy["L"] ** 3 for sy in systems])
+    obs = (nat.Observation * nsys)()
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    nat.check(lib.lj_batch_window_stats(b, W, P(dens), obs))
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        nat.check(lib.lj_batch_window_stats(b, W, P(dens), obs))
+    t_dev = (time.perf_counter() - t0) / reps
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        host = [window_stats_host(recs[:, s, :], systems[s]["N"], dens[s]) for s in range(nsys)]
+    t_host = (time.perf_counter() - t0) / reps
+    rel = max(abs(getattr(obs[s], f) - host[s][f]) / max(abs(host[s][f]), 1e-300)
+              for s in range(nsys) for f, _ in obs[s]._fields_ if f != "density")
+    return {"systems": nsys, "records": W, "device_call_us": 1e6 * t_dev, "host_restatement_us": 1e6 * t_host,
+            "max_rel_diff": rel,
+            "note": "wall clock per call; the device call includes its synchronisation and the copy of the results"}
+
+
 def run_sweep_bench(args):
     """Batched engine vs the same 64 systems run one after another on the GPU: identical
     protocol in both arms (chunks of 200 steps; during the first 2000 steps a system
@@ -486,6 +514,7 @@ def run_sweep_bench(args):
     torch.cuda.synchronize()
     t_batched = time.perf_counter() - t0
     final_batched = recs[-1].copy()
+    wstats = batch_window_stats(lib, b, systems, recs)
     lib.lj_batch_destroy(b)
 
     # sequential, one context at a time
@@ -514,6 +543,7 @@ def run_sweep_bench(args):
                        "list_cells_per_block": tune.list_cells_per_block,
                        "tuned_ms_per_step": tune.ms_per_step, "source": "lj_batch_autotune, 200 steps per candidate"},
             "run_sweep_files": files,
+            "window_stats": wstats,
             "config": {"workload": "8x8 grid rho in [0.05,1.0] x T in [0.5,2.0], N=4n^3, n~U{5..20} (seed 2024), "
                                    "rc=2.5, dt=0.005, 2000 equilibration + 5000 production steps, FP64",
                        "timing": "wall clock around synchronised device work (host decisions included)"}}
@@ -580,6 +610,72 @@ def run_long_bench(args):
                     "max_abs_diff_vs_fp64": float(np.abs(gr["mixed"] - gr["fp64"]).max())},
             "config": {"workload": f"FCC LJ fluid N={N} (4*100^3), rho=0.8, T=0.9, rc=2.5, dt=0.004, seeded MB "
                                    "velocities; RDF 200 bins to 4 sigma every 100 steps", "data": "synthetic"}}
+    print(json.dumps(line), flush=True)
+
+
+OUTPUTS = dict(n_cells=40, T=1.0, rho=0.8442, seed=5489, steps=2000, every=250, window=1000, reps=200)
+
+
+def run_output_bench(args):
+    """The outputs beside the path on one 256 000-atom system (4 * 40^3 FCC, rho
+    0.8442, T 1.0, FP64): the trajectory stream (a frame every 250 of 2000 steps in
+    the snapshot format, written by the background thread while the GPU steps on)
+    against the same 2000 steps without it, by CUDA events on the engine's stream;
+    and the ThermodynamicAnalyzer window statistics over the last 1000 records on
+    the device against the host restatement over the same records."""
+    import tempfile
+    import torch
+    from lennardjonesium import GpuSystem, initial_condition, window_stats_host
+    N = 4 * OUTPUTS["n_cells"] ** 3
+    x, v, L = initial_condition(N, OUTPUTS["T"], OUTPUTS["rho"], OUTPUTS["seed"])
+    steps, W, reps = OUTPUTS["steps"], OUTPUTS["window"], OUTPUTS["reps"]
+    with GpuSystem(N, L) as g:
+        g.upload(x, v=v)
+        g.step(64, record=False)  # graph capture and the first list outside the timed regions
+        stream = torch.cuda.ExternalStream(g.stream)
+
+        def device_seconds(fn):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            g.synchronize()
+            return e0.elapsed_time(e1) / 1e3
+
+        plain = device_seconds(lambda: g.step_async(steps))
+        with tempfile.TemporaryDirectory() as d:
+            path = pathlib.Path(d) / "trajectory.csv"
+            g.trajectory_open(path, OUTPUTS["every"])
+            t0 = time.perf_counter()
+            with_frames = device_seconds(lambda: g.step_async(steps))
+            frames = g.trajectory_close()
+            wall = time.perf_counter() - t0
+            nbytes = path.stat().st_size
+        recs = g.step(W)
+        rho = N / L ** 3
+        dev = g.window_stats(W, rho)
+        host = window_stats_host(recs, N, rho)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            g.window_stats(W, rho)
+        t_dev = (time.perf_counter() - t0) / reps
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            window_stats_host(recs, N, rho)
+        t_host = (time.perf_counter() - t0) / reps
+    rel = max(abs(dev[k] - host[k]) / max(abs(host[k]), 1e-300) for k in dev)
+    line = {"metric": "trajectory stream and window statistics beside the 256 000-atom step",
+            "unit": "ms per step", "value": 1e3 * with_frames / steps, "steps": steps, "atoms": N,
+            "trajectory": {"every": OUTPUTS["every"], "frames": frames, "bytes": nbytes,
+                           "ms_per_step_without": 1e3 * plain / steps, "ms_per_step_with": 1e3 * with_frames / steps,
+                           "device_time_overhead": with_frames / plain - 1.0,
+                           "wall_s_until_written": wall, "rows_per_s": frames * N / wall},
+            "window_stats": {"records": W, "device_call_us": 1e6 * t_dev, "host_restatement_us": 1e6 * t_host,
+                             "max_rel_diff": rel},
+            "config": {"workload": f"FCC LJ fluid N={N} (4*40^3), rho=0.8442, T=1.0, rc=2.5, dt=0.005, FP64; "
+                                   "a frame every 250 of 2000 steps; analyzer over the last 1000 records",
+                       "data": "synthetic"}}
     print(json.dumps(line), flush=True)
 
 
@@ -651,10 +747,11 @@ def main():
     ap.add_argument("--block", type=int, default=0, help="with --no-autotune: pair-kernel block size (default 128)")
     ap.add_argument("--mixed-per-pair", action="store_true",
                     help="mixed path: add every pair force in FP64 (default: FP32 sums of 8 pairs)")
-    ap.add_argument("--workload", choices=("single", "sweep", "long", "adjoint"), default="single",
+    ap.add_argument("--workload", choices=("single", "sweep", "long", "adjoint", "outputs"), default="single",
                     help="single: the 1M-atom benchmark line; sweep: batched vs sequential 64-system sweep; "
                          "long: 4M-atom mixed-precision run with RDF sampling against FP64; "
-                         "adjoint: differentiable NVE gradient at N = 4000")
+                         "adjoint: differentiable NVE gradient at N = 4000; outputs: trajectory stream "
+                         "and window statistics beside the 256 000-atom step")
     ap.add_argument("--long-steps", type=int, default=20000, help="steps of the long workload")
     ap.add_argument("--cells", type=int, default=64,
                     help="FCC cells per box edge (N = 4 cells^3); 64 is the benchmark workload")
@@ -672,6 +769,9 @@ def main():
         return
     if args.workload == "adjoint":
         run_adjoint_bench(args)
+        return
+    if args.workload == "outputs":
+        run_output_bench(args)
         return
     if args.impl == "reference":
         # CPU only: rank 0 runs the reference arm, the other ranks exit at once

@@ -22,6 +22,7 @@
 #include <cstdio>
 #include <cstring>
 #include <deque>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -290,12 +291,16 @@ double relative_error(double measured, double desired) { return std::abs(measure
 namespace ljb {
 
 // Rows of the snapshot file (output/sinks.cpp:185-204): "step,id,x,y,z,vx,vy,vz,fx,fy,fz"
-// for atoms 0..n-1 of xvf (9 doubles per atom).  Returns 0, or 1 if a write failed.
-int write_snapshot_rows(long long time_step, const double* xvf, int n, FILE* f) {
-    std::vector<char> buf;
-    buf.reserve(1 << 20);
+// for atoms 0..n-1 of xvf (9 doubles per atom).  Large frames are formatted in
+// blocks of kSnapshotBlock rows on up to 16 threads at a time and written in
+// row order (a 256 000-atom frame is ~50 MB of text; one thread formats ~2 M
+// rows per second).  Returns 0, or 1 if a write failed.
+constexpr int kSnapshotBlock = 32768;
+
+static void format_snapshot_block(long long time_step, const double* xvf, int lo, int hi, std::vector<char>& buf) {
+    buf.clear();
     char line[400];
-    for (int i = 0; i < n; ++i) {
+    for (int i = lo; i < hi; ++i) {
         char* o = line;
         o = std::to_chars(o, o + 24, time_step).ptr;
         *o++ = ',';
@@ -306,12 +311,27 @@ int write_snapshot_rows(long long time_step, const double* xvf, int n, FILE* f) 
         }
         *o++ = '\n';
         buf.insert(buf.end(), line, o);
-        if (buf.size() > (1 << 20) - 512) {
-            if (std::fwrite(buf.data(), 1, buf.size(), f) != buf.size()) return 1;
-            buf.clear();
+    }
+}
+
+int write_snapshot_rows(long long time_step, const double* xvf, int n, FILE* f) {
+    unsigned hw = std::thread::hardware_concurrency();
+    int P = (int)std::min(16u, std::max(1u, hw));
+    std::vector<std::vector<char>> bufs((size_t)P);
+    for (int base = 0; base < n; base += P * kSnapshotBlock) {
+        int nb = std::min(P, (n - base + kSnapshotBlock - 1) / kSnapshotBlock);
+        std::vector<std::thread> th;
+        for (int b = 1; b < nb; ++b) {
+            int lo = base + b * kSnapshotBlock, hi = std::min(n, lo + kSnapshotBlock);
+            th.emplace_back(format_snapshot_block, time_step, xvf, lo, hi, std::ref(bufs[(size_t)b]));
+        }
+        format_snapshot_block(time_step, xvf, base, std::min(n, base + kSnapshotBlock), bufs[0]);
+        for (std::thread& t : th) t.join();
+        for (int b = 0; b < nb; ++b) {
+            const std::vector<char>& q = bufs[(size_t)b];
+            if (!q.empty() && std::fwrite(q.data(), 1, q.size(), f) != q.size()) return 1;
         }
     }
-    if (!buf.empty() && std::fwrite(buf.data(), 1, buf.size(), f) != buf.size()) return 1;
     return std::fflush(f) == 0 ? 0 : 1;
 }
 

@@ -7,7 +7,7 @@ Simulations run on a CUDA engine reached through the C ABI of include/lj_gpu.h;
 GpuSystem exposes that engine directly.
 """
 
-from lennardjonesium.engine import GpuSystem, initial_condition, autotune, THERMO_FIELDS
+from lennardjonesium.engine import GpuSystem, initial_condition, autotune, window_stats_host, THERMO_FIELDS
 from lennardjonesium.simulation import SeedGenerator, Configuration, Simulation, SimulationPool
 from lennardjonesium.orchestration import run, run_sweep, SweepConfiguration, SweepResult, RunResult
 

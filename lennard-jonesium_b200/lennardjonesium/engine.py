@@ -33,6 +33,16 @@ def _as4(a, N):
     return out
 
 
+def window_stats_host(records, particle_count, density):
+    """The same analysis as GpuSystem.window_stats on records the caller holds
+    ((n, 7) step records, oldest first), in the reference's summation order."""
+    r = np.ascontiguousarray(records, dtype=np.float64)
+    o = nat.Observation()
+    nat.check(nat.lib().lj_window_stats_host(_p(r), r.shape[0], int(particle_count), float(density),
+                                             ctypes.byref(o)))
+    return {f: getattr(o, f) for f, _ in o._fields_}
+
+
 def lattice_side(N, density):
     """Edge of the cubic box engine::InitialCondition builds (tools/cubic_lattice.cpp:43-58)."""
     import math
@@ -243,6 +253,15 @@ class GpuSystem:
         n = ctypes.c_longlong()
         self._check(nat.lib().lj_gpu_trajectory_close(self._ctx, ctypes.byref(n)))
         return n.value
+
+    def window_stats(self, sample_size, density):
+        """ThermodynamicAnalyzer result (physics/analyzers.cpp:44-159) over the last
+        sample_size step records, computed on the device from the record ring:
+        temperature, density, total_energy, pressure, specific_heat,
+        diffusion_coefficient."""
+        o = nat.Observation()
+        self._check(nat.lib().lj_gpu_window_stats(self._ctx, int(sample_size), float(density), ctypes.byref(o)))
+        return {f: getattr(o, f) for f, _ in o._fields_}
 
     def stats(self):
         s = nat.Stats()

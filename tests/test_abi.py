@@ -213,3 +213,6 @@ def test_window_stats_host_matches_the_analyzer_formulas():
             1.5 / (1 - 1.5 * N * varT / T ** 2), np.cov(rec[:, 0], rec[:, 6])[0, 1] / rec[:, 0].var(ddof=1) / 6]
     got = [getattr(o, f) for f, _ in o._fields_]
     assert np.allclose(got, want, rtol=1e-12, atol=0)
+    # the package's wrapper returns the same fields by name
+    from lennardjonesium import window_stats_host
+    assert list(window_stats_host(rec, N, rho).values()) == got

@@ -145,6 +145,27 @@ def test_trajectory_frames_equal_downloads(tmp_path, precision):
     assert path.read_text() == "\n".join(want) + "\n"
 
 
+def test_trajectory_frame_of_a_large_system(tmp_path):
+    """A frame of 42 592 atoms, more than one formatting block of 32 768 rows (the
+    blocks are formatted on parallel threads and written in row order), is byte
+    for byte the snapshot rows of lj_gpu_download_state at that step."""
+    from lennardjonesium import GpuSystem
+    N = 4 * 22 ** 3
+    x, v, L = ljref.initial_state(N, 1.0, 0.8442, 11)
+    path = tmp_path / "trajectory.csv"
+    with GpuSystem(N, L) as g:
+        g.upload(x, v=v)
+        g.trajectory_open(path, 5)
+        g.step(5, record=False)
+        st = g.download()
+        assert g.trajectory_close() == 1
+    lines = path.read_text().split("\n")
+    assert len(lines) == 2 + N + 1 and lines[-1] == ""
+    for i in range(N):
+        vals = [st[k][i, q] for k in ("x", "v", "F") for q in range(3)]
+        assert lines[2 + i] == ",".join(["5", str(i)] + [_fmt(a) for a in vals]), i
+
+
 def test_equilibration_reaches_a_new_temperature():
     """tests/cpp/integration/test_system_equilibration.cpp, loose phase: N = 100 at
     rho 0.8, rc 2.0 (two list cells per axis), started at T 0.3 and driven to 0.8

@@ -192,6 +192,21 @@ def test_context_window_statistics_on_device():
         assert nat.lib().lj_gpu_window_stats(g._ctx, 1025, 0.8, ctypes.byref(o)) == nat.LJ_ERR_ARG
 
 
+def test_window_stats_through_the_python_api():
+    """GpuSystem.window_stats (device) equals window_stats_host over the records
+    step() returned, to 1e-12."""
+    from lennardjonesium import GpuSystem, window_stats_host
+    x, v, L = ljref.initial_state(4000, 1.2, 0.8, 7)
+    with GpuSystem(4000, L) as g:
+        g.upload(x, v=v)
+        recs = g.step(600)
+        dev = g.window_stats(500, 0.8)
+    host = window_stats_host(recs[-500:], 4000, 0.8)
+    assert dev.keys() == host.keys()
+    for k in host:
+        assert abs(dev[k] - host[k]) <= 1e-12 * abs(host[k]), (k, dev[k], host[k])
+
+
 def test_batch_chunk_loop_bound():
     """A chunk launch runs its device-side loop under an iteration bound: with the
     bound set below the chunk's 8 iterations the launch stops early and the call
