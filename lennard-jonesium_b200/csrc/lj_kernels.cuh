@@ -331,32 +331,24 @@ build_list_kernel(int N, const double4* __restrict__ pos, const float4* __restri
 // add / multiply / fma, in unrolled blocks of 8 that only set bits of a hit
 // mask.  The masks of up to kBuildRecords chunks are kept in shared memory
 // (with each chunk's first slot, entry code and the slots where the code's z
-// offset steps up) and then appended in one per-lane loop over all their set
-// bits: the warp runs as many append rounds as its busiest lane has hits,
-// instead of the busiest lane's hits in every chunk added up.  Each lane
-// collects entries in a 4-entry shared buffer and writes whole groups (one
-// 16-byte store).  Entries, their order (stencil cell, then slot) and the
-// candidate radius are those of build_list_kernel<false>.  The per-cell body,
-// build_cell_lists, also serves the batched engine's list build.
+// offset steps up) and then appended in one loop over all their set bits: the
+// warp runs as many append rounds as its busiest lane has hits (a warp-uniform
+// count), instead of the busiest lane's hits in every chunk added up.  In a
+// round every lane with hits left appends one entry, first moving on to its
+// next record with hits when its current mask is empty (a per-lane bit set of
+// the records with hits, so the walk takes no divergent loop), and writes the
+// entry with one 4-byte store.  Entries, their order (stencil cell, then slot)
+// and the candidate radius are those of build_list_kernel<false>.  The
+// per-cell body, build_cell_lists, also serves the batched engine's list build.
 constexpr int kBuildWarps = 4;
-constexpr int kBuildRecords = 24;
+constexpr int kBuildRecords = 24;  // <= 32: bits of a lane's record set
 
-__device__ __forceinline__ void append_entry(unsigned (&grp)[4], int& n, int cap, unsigned entry,
-                                             uint4* __restrict__ nbr4, size_t N, int i) {
-    if (n < cap) {
-        grp[n & 3] = entry;
-        if ((n & 3) == 3) nbr4[(size_t)(n >> 2) * N + i] = make_uint4(grp[0], grp[1], grp[2], grp[3]);
-    }
-    ++n;
-}
-
-// Shared memory of one list-building warp: the staged candidates, each lane's
-// 4-entry group buffer and the chunk records waiting to be appended (per
-// chunk: first slot, entry code of its first cell, slots where the z offset
-// of the code steps up by one -- INT_MAX: none).
+// Shared memory of one list-building warp: the staged candidates and the
+// chunk records waiting to be appended (per chunk: first slot, entry code of
+// its first cell, slots where the z offset of the code steps up by one --
+// INT_MAX: none).
 struct __align__(16) BuildSmem {
     float cxs[3][32];
-    unsigned grp[32][4];
     unsigned rec_mask[kBuildRecords][32];
     int4 rec_meta[kBuildRecords];
 };
@@ -370,7 +362,7 @@ __device__ __forceinline__ int build_cell_lists(int ca, int cb, int cc, const Gr
                                                 uint4* __restrict__ nbr4, int* __restrict__ cnt, int N,
                                                 BuildSmem& sm, int lane) {
     int wmax = 0;
-    unsigned(&grp)[4] = sm.grp[lane];
+    unsigned* const list = reinterpret_cast<unsigned*>(nbr4);  // entry q of group g of slot i: (g*N + i)*4 + q
     int nz = g.n[2];
     // the column's z cells d = -1, 0, 1 as at most two contiguous pieces,
     // split where the column wraps (each piece has one z image)
@@ -388,29 +380,36 @@ __device__ __forceinline__ int build_cell_lists(int ca, int cb, int cc, const Gr
         bool own = i < he;
         float4 xi = own ? posf[i] : make_float4(0.f, 0.f, 0.f, 0.f);
         int n = 0;
-        int nrec = 0;  // chunk records waiting to be appended (warp-uniform)
-        // append the hits of the recorded chunks in order: one round per hit
-        // of this lane, a round that finds the current mask empty first moves
-        // on to the next record
+        int nrec = 0;     // chunk records waiting to be appended (warp-uniform)
+        unsigned ne = 0;  // this lane's waiting records with hits (bit k: record k)
+        int pend = 0;     // this lane's hits in the waiting records
+        // append the hits of the recorded chunks in order, one per lane and
+        // round, for as many rounds as the busiest lane has hits
         auto flush = [&]() {
             __syncwarp();
-            int k = 0;
-            unsigned m = sm.rec_mask[0][lane];
-            int4 meta = sm.rec_meta[0];
-            for (;;) {
-                while (m == 0 && ++k < nrec) {
+            int rounds = __reduce_max_sync(0xffffffffu, pend);
+            unsigned m = 0;
+            int4 meta = make_int4(0, 0, INT_MAX, INT_MAX);
+            unsigned* const row = list + (size_t)i * 4;
+            for (int r = 0; r < rounds; ++r) {
+                if (m == 0 && ne != 0) {
+                    int k = __ffs(ne) - 1;
+                    ne &= ne - 1;
                     m = sm.rec_mask[k][lane];
                     meta = sm.rec_meta[k];
                 }
-                if (m == 0) break;
-                int t = __clz(m);
-                m ^= 0x80000000u >> t;
-                int j = meta.x + t;
-                unsigned code = (unsigned)meta.y + (j >= meta.z ? 16u : 0u) + (j >= meta.w ? 16u : 0u);
-                append_entry(grp, n, cap, make_entry((unsigned)j, code), nbr4, N, i);
+                if (m != 0) {
+                    int t = __clz(m);
+                    m ^= 0x80000000u >> t;
+                    int j = meta.x + t;
+                    unsigned code = (unsigned)meta.y + (j >= meta.z ? 16u : 0u) + (j >= meta.w ? 16u : 0u);
+                    if (n < cap) row[(size_t)(n >> 2) * N * 4 + (n & 3)] = make_entry((unsigned)j, code);
+                    ++n;
+                }
             }
             __syncwarp();
             nrec = 0;
+            pend = 0;
         };
         for (int a = -1; a <= 1; ++a) {
             int na = ca + a, ia = na < 0 ? -1 : (na >= g.n[0] ? 1 : 0);
@@ -467,6 +466,8 @@ __device__ __forceinline__ int build_cell_lists(int ca, int cb, int cc, const Gr
                         if (!own) mask = 0;
                         if (__any_sync(0xffffffffu, mask != 0u)) {
                             sm.rec_mask[nrec][lane] = mask;
+                            ne |= (mask != 0u ? 1u : 0u) << nrec;
+                            pend += __popc(mask);
                             if (lane == 0) {
                                 // the piece's z offsets: slot j lies in the cell
                                 // d = pd0 + (j >= s0 if the piece holds d = 0) + ...
@@ -485,10 +486,8 @@ __device__ __forceinline__ int build_cell_lists(int ca, int cb, int cc, const Gr
         if (own) {
             int m = n < cap ? n : cap;
             cnt[i] = m;
-            if (m & 3) {  // pad the last group with the ghost slot
-                for (int k = m & 3; k < 4; ++k) grp[k] = make_entry((unsigned)N, kGhostCode);
-                nbr4[(size_t)(m >> 2) * N + i] = make_uint4(grp[0], grp[1], grp[2], grp[3]);
-            }
+            for (int k = m; k < ((m + 3) & ~3); ++k)  // pad the last group with the ghost slot
+                list[((size_t)(k >> 2) * N + i) * 4 + (k & 3)] = make_entry((unsigned)N, kGhostCode);
             wmax = max(wmax, n);
         }
     }
