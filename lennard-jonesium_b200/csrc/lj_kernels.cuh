@@ -344,9 +344,9 @@ constexpr int kBuildWarps = 4;
 constexpr int kBuildRecords = 24;  // <= 32: bits of a lane's record set
 
 // Shared memory of one list-building warp: the staged candidates and the
-// chunk records waiting to be appended (per chunk: first slot, entry code of
-// its first cell, slots where the z offset of the code steps up by one --
-// INT_MAX: none).
+// chunk records waiting to be appended (per chunk: the entry of its first
+// candidate, and the candidate indices within the chunk from which the z
+// offset of the code is one and two steps up -- INT_MAX: none).
 struct __align__(16) BuildSmem {
     float cxs[3][32];
     unsigned rec_mask[kBuildRecords][32];
@@ -390,7 +390,10 @@ __device__ __forceinline__ int build_cell_lists(int ca, int cb, int cc, const Gr
             int rounds = __reduce_max_sync(0xffffffffu, pend);
             unsigned m = 0;
             int4 meta = make_int4(0, 0, INT_MAX, INT_MAX);
-            unsigned* const row = list + (size_t)i * 4;
+            // the entry slot of this lane's next entry, stepped per append
+            // (entry q + 1 of a group, or entry 0 of the next group N*4 - 3 on)
+            unsigned* p = list + ((size_t)(n >> 2) * N + i) * 4 + (n & 3);
+            const size_t next_group = (size_t)N * 4 - 3;
             for (int r = 0; r < rounds; ++r) {
                 if (m == 0 && ne != 0) {
                     int k = __ffs(ne) - 1;
@@ -401,9 +404,12 @@ __device__ __forceinline__ int build_cell_lists(int ca, int cb, int cc, const Gr
                 if (m != 0) {
                     int t = __clz(m);
                     m ^= 0x80000000u >> t;
-                    int j = meta.x + t;
-                    unsigned code = (unsigned)meta.y + (j >= meta.z ? 16u : 0u) + (j >= meta.w ? 16u : 0u);
-                    if (n < cap) row[(size_t)(n >> 2) * N * 4 + (n & 3)] = make_entry((unsigned)j, code);
+                    // entry of candidate j0 + t: the record's first entry plus t slots,
+                    // plus one z step of the code per cell boundary passed
+                    unsigned e = (unsigned)meta.x + ((unsigned)t << kCodeBits) + (t >= meta.y ? 16u : 0u) +
+                                 (t >= meta.z ? 16u : 0u);
+                    if (n < cap) *p = e;
+                    p += (n & 3) == 3 ? next_group : 1;
                     ++n;
                 }
             }
@@ -473,8 +479,9 @@ __device__ __forceinline__ int build_cell_lists(int ca, int cb, int cc, const Gr
                                 // d = pd0 + (j >= s0 if the piece holds d = 0) + ...
                                 int dl = pd0[pc], dh = pd1[pc];
                                 sm.rec_meta[nrec] =
-                                    make_int4(j0, (int)offset_code(a, b, dl), dl < 0 && dh >= 0 ? s0 : INT_MAX,
-                                              dl < 1 && dh >= 1 ? s1 : INT_MAX);
+                                    make_int4((int)make_entry((unsigned)j0, offset_code(a, b, dl)),
+                                              dl < 0 && dh >= 0 ? s0 - j0 : INT_MAX,
+                                              dl < 1 && dh >= 1 ? s1 - j0 : INT_MAX, 0);
                             }
                             if (++nrec == kBuildRecords) flush();
                         }
