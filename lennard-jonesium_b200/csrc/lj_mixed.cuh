@@ -34,7 +34,8 @@ struct MixedParams {
     float rc2, inv_rc2, alpha, beta;
     float a[3];  // list-cell edge per axis
     // the spline's virial as a function of r^2: W = u(48u - 24) + wq r^2 with
-    // u = r^-6 (lennard_jones_force.cpp:107-119)
+    // u = r^-6 (lennard_jones_force.cpp:107-119), so the force magnitude over r
+    // is f = W / r^2 = u(48u - 24) r^-2 + wq
     float wq;
 };
 
@@ -138,8 +139,8 @@ force_mixed_kernel(int N, const float4* __restrict__ posl, Soa s, const uint4* _
                 bool hit = r2 < mp.rc2;
                 float ir2 = rcp_approx(r2);
                 float ir6 = ir2 * ir2 * ir2;
-                float W = fmaf(ir6, fmaf(48.f, ir6, -24.f), mp.wq * r2);
-                float f = hit ? W * ir2 : 0.f;
+                // f = W / r^2 = u(48u - 24) r^-2 + wq
+                float f = hit ? fmaf(ir6 * fmaf(48.f, ir6, -24.f), ir2, mp.wq) : 0.f;
                 float uh = hit ? ir6 : 0.f;
                 float rh = hit ? r2 : 0.f;
                 nh += hit ? 1 : 0;
