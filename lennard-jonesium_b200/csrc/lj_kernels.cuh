@@ -330,16 +330,17 @@ build_list_kernel(int N, const double4* __restrict__ pos, const float4* __restri
 // through broadcast reads, two per instruction with Blackwell's packed FP32x2
 // add / multiply / fma, in unrolled blocks of 8 that only set bits of a hit
 // mask.  The masks of up to kBuildRecords chunks are kept in shared memory
-// (with each chunk's first slot, entry code and the slots where the code's z
-// offset steps up) and then appended in one loop over all their set bits: the
-// warp runs as many append rounds as its busiest lane has hits (a warp-uniform
-// count), instead of the busiest lane's hits in every chunk added up.  In a
-// round every lane with hits left appends one entry, first moving on to its
-// next record with hits when its current mask is empty (a per-lane bit set of
-// the records with hits, so the walk takes no divergent loop), and writes the
-// entry with one 4-byte store.  Entries, their order (stencil cell, then slot)
-// and the candidate radius are those of build_list_kernel<false>.  The
-// per-cell body, build_cell_lists, also serves the batched engine's list build.
+// (with the entry of each chunk's first candidate and the candidates from
+// which the code's z offset steps up) and then appended in one loop over all
+// their set bits: the warp runs as many append rounds as its busiest lane has
+// hits (a warp-uniform count), instead of the busiest lane's hits in every
+// chunk added up.  In a round every lane with hits left appends one entry,
+// first moving on to its next record with hits when its current mask is empty
+// (a per-lane bit set of the records with hits, so the walk takes no divergent
+// loop), and writes the entry with one 4-byte store through a pointer stepped
+// per append.  Entries, their order (stencil cell, then slot) and the
+// candidate radius are those of build_list_kernel<false>.  The per-cell body,
+// build_cell_lists, also serves the batched engine's list build.
 constexpr int kBuildWarps = 4;
 constexpr int kBuildRecords = 24;  // <= 32: bits of a lane's record set
 
