@@ -444,7 +444,10 @@ __device__ __forceinline__ int build_cell_lists(int ca, int cb, int cc, const Gr
                         sm.cxs[2][lane] = -q.z;
                         __syncwarp();
                         unsigned mask = 0;
-                        for (int t0 = 0; t0 < cntj; t0 += 8) {
+                        // the four blocks of 8 unrolled, cut short past the range
+#pragma unroll
+                        for (int t0 = 0; t0 < 32; t0 += 8) {
+                            if (t0 >= cntj) break;
                             // r2 < cut2 exactly when r2 - cut2 is negative: its sign bit
                             // is shifted into `sub`, first candidate highest
                             unsigned sub = 0;
