@@ -348,6 +348,18 @@ b_finalize_kernel(const SysDev* __restrict__ sys, SysState* st, int nsys, const 
     const SysDev& S = sys[sidx];
     SysState& T = st[sidx];
     if (mode == 0 && !T.active) return;
+    // thread 0 loads the state it updates before the reduction, so that those
+    // loads overlap the partials' (only this block changes them while it runs)
+    double t0 = 0, pe0 = 0, vir0 = 0;
+    long long steps0 = 0;
+    int slot = 0;
+    if (threadIdx.x == 0) {
+        t0 = T.t;
+        pe0 = T.pe;
+        vir0 = T.vir;
+        steps0 = T.steps;
+        slot = fl->slot;
+    }
     double acc[4] = {0, 0, 0, 0};
     int off = mode == 2 ? S.blk_off : S.fblk_off, nb = mode == 2 ? S.nblk : S.nfblk;
     for (int b = threadIdx.x; b < nb; b += blockDim.x)
@@ -355,26 +367,30 @@ b_finalize_kernel(const SysDev* __restrict__ sys, SysState* st, int nsys, const 
         for (int q = 0; q < 4; ++q) acc[q] += partials[(size_t)(off + b) * 4 + q];
     block_sum<4, 1024>(acc);
     if (threadIdx.x == 0) {
+        double pe = pe0, vir = vir0, t = t0;
         if (mode != 2) {
-            T.pe = 0.5 * acc[1];
-            T.vir = 0.5 * acc[2];
+            pe = 0.5 * acc[1];
+            vir = 0.5 * acc[2];
+            T.pe = pe;
+            T.vir = vir;
         }
-        double* out = ring + 7 * ((size_t)(mode == 0 ? fl->slot : ring_cap) * nsys + sidx);
+        double* out = ring + 7 * ((size_t)(mode == 0 ? slot : ring_cap) * nsys + sidx);
         if (mode == 0) {
-            T.t = T.t + S.pp.dt;
-            T.steps += 1;
+            t = t0 + S.pp.dt;
+            T.t = t;
+            T.steps = steps0 + 1;
         }
         double ke = 0.5 * acc[0];
         if (mode != 1) {
-            out[0] = T.t;
+            out[0] = t;
             out[1] = ke;
-            out[2] = T.pe;
-            out[3] = T.pe + ke;
-            out[4] = T.vir;
+            out[2] = pe;
+            out[3] = pe + ke;
+            out[4] = vir;
             out[5] = (2. / 3.) * ke / (double)S.natoms;
             out[6] = acc[3] / (double)S.natoms;
         }
-        if (!isfinite(ke) || !isfinite(T.pe) || !isfinite(T.vir)) atomicExch(&fl->nonfinite, 1);
+        if (!isfinite(ke) || !isfinite(pe) || !isfinite(vir)) atomicExch(&fl->nonfinite, 1);
         if (mode == 0) {
             T.max_disp2 = 0ull;
             T.need_rebuild = 0;

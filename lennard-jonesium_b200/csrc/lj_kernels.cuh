@@ -786,6 +786,23 @@ struct NextStep {
 static __global__ void __launch_bounds__(1024)
 finalize_kernel(const double* __restrict__ partials, int nblocks, int N, double dt, int mode,
                 int forces_valid, Scalars* sc, double* __restrict__ ring, int ring_cap, NextStep next) {
+    // thread 0 loads the scalars it updates before the reduction, so that those
+    // loads overlap the partials' instead of following one another at the end
+    // (only this kernel changes them while it runs)
+    double t0 = 0, pe0 = 0, vir0 = 0;
+    long long steps0 = 0, rebuilds0 = 0;
+    unsigned long long md2_0 = 0, md2_next = 0;
+    int need0 = 0;
+    if (threadIdx.x == 0) {
+        t0 = sc->t;
+        pe0 = sc->pe;
+        vir0 = sc->vir;
+        steps0 = sc->steps;
+        rebuilds0 = sc->graph_rebuilds;
+        md2_0 = sc->max_disp2;
+        md2_next = sc->max_disp2_next;
+        need0 = sc->need_rebuild;
+    }
     // each thread sums blocks tid, tid + 1024, ... in that order; eight blocks'
     // partials (32-byte loads) are in flight at a time
     double acc[4] = {0, 0, 0, 0};
@@ -809,41 +826,50 @@ finalize_kernel(const double* __restrict__ partials, int nblocks, int N, double 
     }
     block_sum<4, 1024>(acc);
     if (threadIdx.x == 0) {
+        double pe = pe0, vir = vir0, t = t0;
         if (forces_valid) {
-            sc->pe = 0.5 * acc[1];
-            sc->vir = 0.5 * acc[2];
+            pe = 0.5 * acc[1];
+            vir = 0.5 * acc[2];
+            sc->pe = pe;
+            sc->vir = vir;
         }
         // a step's record goes to ring slot (step index mod ring_cap); the extra
         // slot ring_cap holds single measurements
-        double* out = ring + 7 * (size_t)(mode == 0 ? (int)(sc->steps % ring_cap) : ring_cap);
+        double* out = ring + 7 * (size_t)(mode == 0 ? (int)(steps0 % ring_cap) : ring_cap);
         if (mode == 0) {
-            sc->t = sc->t + dt;  // integrator.cpp:85
-            sc->steps += 1;
+            t = t0 + dt;  // integrator.cpp:85
+            sc->t = t;
+            sc->steps = steps0 + 1;
         }
         if (mode != 1) {
             double ke = 0.5 * acc[0];
             double rec[7];
-            rec[0] = sc->t;
+            rec[0] = t;
             rec[1] = ke;
-            rec[2] = sc->pe;
-            rec[3] = sc->pe + ke;
-            rec[4] = sc->vir;
+            rec[2] = pe;
+            rec[3] = pe + ke;
+            rec[4] = vir;
             rec[5] = (2. / 3.) * ke / (double)N;
             rec[6] = acc[3] / (double)N;
             for (int q = 0; q < 7; ++q) out[q] = rec[q];
-            if (!isfinite(ke) || !isfinite(sc->pe) || !isfinite(sc->vir)) sc->nonfinite = 1;
-        } else if (!isfinite(sc->pe) || !isfinite(sc->vir)) {
+            if (!isfinite(ke) || !isfinite(pe) || !isfinite(vir)) sc->nonfinite = 1;
+        } else if (!isfinite(pe) || !isfinite(vir)) {
             sc->nonfinite = 1;
         }
+        unsigned long long md2 = md2_0;
+        int need = need0;
         if (mode != 2) {  // a measurement changes nothing that a rebuild depends on
             // the next step's displacement (a fused epilogue's, else 0 for kick_drift)
-            sc->max_disp2 = sc->max_disp2_next;
+            md2 = md2_next;
+            need = 0;
+            sc->max_disp2 = md2;
             sc->max_disp2_next = 0ull;
             sc->need_rebuild = 0;
         }
         if (next.set) {
-            bool open = next.gate.open();
-            if (open) sc->graph_rebuilds += 1;
+            // next.gate.open() on the values just written
+            bool open = next.gate.always || need || __longlong_as_double((long long)md2) > next.gate.thresh2;
+            if (open) sc->graph_rebuilds = rebuilds0 + 1;
             cudaGraphSetConditional(next.h, open ? 1u : 0u);
         }
     }
