@@ -212,7 +212,8 @@ int lj_window_stats_host(const lj_thermo* records, int n, int particle_count, do
  * completes a step whose count (steps this context has taken) is a multiple
  * of `every`, that state's frame is copied to pinned host memory on the
  * context's stream and written by a background thread while the GPU runs on
- * (two frames in flight at most).  lj_gpu_trajectory_close waits for every
+ * (two frames in flight at most; frames above 32 768 atoms are formatted in
+ * blocks on up to 16 short-lived threads and written in row order).  lj_gpu_trajectory_close waits for every
  * frame, closes the file and reports how many frames it holds (may be NULL).
  * lj_gpu_destroy closes an open trajectory. */
 int lj_gpu_trajectory_open(lj_ctx* ctx, const char* path, int every);
